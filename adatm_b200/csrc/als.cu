@@ -1,0 +1,488 @@
+// als.cu -- dense CP-ALS kernels (see als.cuh).
+#include <algorithm>
+
+#include "als.cuh"
+
+namespace adatm {
+
+namespace {
+void set_attributes();
+}
+
+void AlsWork::init(int nmodes_, int R_, int nblocks_, int max_iters) {
+  nmodes = nmodes_;
+  R = R_;
+  ldr = ldr_of(R_);
+  nblocks = nblocks_;
+  vinv64.alloc((size_t)R * R);
+  vinv32.alloc((size_t)R * R);
+  part_gram.alloc((size_t)nblocks * R * R);
+  part_max.alloc((size_t)nblocks * R);
+  part_inner.alloc((size_t)nblocks * R);
+  lambda.alloc(R);
+  scalars.alloc(8);
+  iter.alloc(1);
+  max_trace = std::max(1, max_iters);
+  fit_trace.alloc(max_trace);
+  ADATM_CUDA(cudaMemset(scalars.get(), 0, 8 * sizeof(double)));
+  ADATM_CUDA(cudaMemset(iter.get(), 0, sizeof(int)));
+  ADATM_CUDA(cudaMemset(fit_trace.get(), 0, max_trace * sizeof(double)));
+  set_attributes();
+}
+
+namespace {
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void k_factor_init(float *A, __nv_bfloat16 *Ab, uint64_t rows, int R, int ldr,
+                              uint64_t key) {
+  const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= rows * (uint64_t)ldr) return;
+  const uint64_t i = e / ldr;
+  const int r = (int)(e % ldr);
+  float v = 0.f;
+  if (r < R) {
+    const uint64_t x = i * (uint64_t)R + r;
+    v = (float)((double)(mix64(key + x) >> 11) * (1.0 / 9007199254740992.0));
+  }
+  A[e] = v;
+  if (Ab) Ab[e] = __float2bfloat16(v);
+}
+
+__global__ void k_to_bf16(const float *A, __nv_bfloat16 *Ab, uint64_t n) {
+  const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) Ab[e] = __float2bfloat16(A[e]);
+}
+
+constexpr int kFrobThreads = 256;
+
+__global__ void k_frob_partial(const double *v, uint64_t n, double *part) {
+  double s = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    s += v[i] * v[i];
+  __shared__ double red[kFrobThreads];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = kFrobThreads / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+__global__ void k_frob_final(const double *part, int n, double *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < n; ++i) s += part[i];
+    out[0] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gram Hadamard + Cholesky + inverse, one block.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int mode, int R,
+                                                      double *X, float *X32) {
+  extern __shared__ double L[];  // R x R
+  const int tid = threadIdx.x;
+  for (int e = tid; e < R * R; e += blockDim.x) {
+    double v = 1.0;
+    for (int m = 0; m < nmodes; ++m)
+      if (m != mode) v *= g.G[m][e];
+    L[e] = v;
+  }
+  __syncthreads();
+  // right-looking Cholesky, lower triangle in place
+  for (int j = 0; j < R; ++j) {
+    if (tid == 0) L[j * R + j] = sqrt(L[j * R + j]);
+    __syncthreads();
+    const double djj = L[j * R + j];
+    for (int i = j + 1 + tid; i < R; i += blockDim.x) L[i * R + j] /= djj;
+    __syncthreads();
+    const int rest = R - j - 1;
+    for (int e = tid; e < rest * rest; e += blockDim.x) {
+      const int i = j + 1 + e / rest, k = j + 1 + e % rest;
+      if (k <= i) L[i * R + k] -= L[i * R + j] * L[k * R + j];
+    }
+    __syncthreads();
+  }
+  // column c of the inverse: forward solve L y = e_c, backward L^T x = y
+  for (int c = tid; c < R; c += blockDim.x) {
+    for (int i = 0; i < R; ++i) {
+      double t = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) t -= L[i * R + k] * X[k * R + c];
+      X[i * R + c] = t / L[i * R + i];
+    }
+    for (int i = R - 1; i >= 0; --i) {
+      double t = X[i * R + c];
+      for (int k = i + 1; k < R; ++k) t -= L[k * R + i] * X[k * R + c];
+      X[i * R + c] = t / L[i * R + i];
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < R * R; e += blockDim.x) X32[e] = (float)X[e];
+}
+
+// ---------------------------------------------------------------------------
+// Row update A_raw = M * Vinv (or A_raw = M when vinv == nullptr), with
+// per-block FP64 partial Gram and column maxima of A_raw.
+// ---------------------------------------------------------------------------
+struct UpdArgs {
+  const float *M;
+  const float *vinv;  // R x R fp32, or nullptr for identity
+  float *A;           // output rows (may alias M when vinv == nullptr)
+  uint64_t rows;
+  int R, ldr;
+  double *part_gram;  // gridDim x R x R
+  double *part_max;   // gridDim x R
+};
+
+template <int LANES>
+__global__ void __launch_bounds__(256) k_update(UpdArgs a) {
+  constexpr int GROUPS = 256 / LANES;
+  constexpr int RMAX = 4 * LANES;
+  constexpr int PAIRS = (RMAX * RMAX + 255) / 256;
+  extern __shared__ float usm[];
+  float *vinv = usm;                      // RMAX x RMAX
+  float *rowbuf = usm + RMAX * RMAX;      // GROUPS x RMAX
+  const int tid = threadIdx.x;
+  const int g = tid / LANES, t = tid % LANES, col = 4 * t;
+  const int R = a.R;
+  const bool act = col < R;
+  const unsigned gmask =
+      LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << ((tid & 31) / LANES * LANES));
+  if (a.vinv) {
+    for (int e = tid; e < RMAX * RMAX; e += 256) {
+      const int k = e / RMAX, c = e % RMAX;
+      vinv[e] = (k < R && c < R) ? a.vinv[k * R + c] : 0.f;
+    }
+  }
+  double gacc[PAIRS];
+#pragma unroll
+  for (int p = 0; p < PAIRS; ++p) gacc[p] = 0.0;
+  double cmax = 0.0;
+  __syncthreads();
+  const int kq = (R + 3) / 4;
+  for (uint64_t row0 = (uint64_t)blockIdx.x * GROUPS; row0 < a.rows;
+       row0 += (uint64_t)gridDim.x * GROUPS) {
+    const uint64_t i = row0 + g;
+    const bool valid = i < a.rows;
+    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (valid && act) m = *reinterpret_cast<const float4 *>(a.M + i * a.ldr + col);
+    float4 o;
+    if (a.vinv) {
+      o = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int kk = 0; kk < kq; ++kk) {
+        const float m0 = __shfl_sync(gmask, m.x, kk, LANES);
+        const float m1 = __shfl_sync(gmask, m.y, kk, LANES);
+        const float m2 = __shfl_sync(gmask, m.z, kk, LANES);
+        const float m3 = __shfl_sync(gmask, m.w, kk, LANES);
+        const float4 v0 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 0) * RMAX + col);
+        const float4 v1 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 1) * RMAX + col);
+        const float4 v2 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 2) * RMAX + col);
+        const float4 v3 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 3) * RMAX + col);
+        o.x = fmaf(m0, v0.x, fmaf(m1, v1.x, fmaf(m2, v2.x, fmaf(m3, v3.x, o.x))));
+        o.y = fmaf(m0, v0.y, fmaf(m1, v1.y, fmaf(m2, v2.y, fmaf(m3, v3.y, o.y))));
+        o.z = fmaf(m0, v0.z, fmaf(m1, v1.z, fmaf(m2, v2.z, fmaf(m3, v3.z, o.z))));
+        o.w = fmaf(m0, v0.w, fmaf(m1, v1.w, fmaf(m2, v2.w, fmaf(m3, v3.w, o.w))));
+      }
+      if (valid && act) *reinterpret_cast<float4 *>(a.A + i * a.ldr + col) = o;
+    } else {
+      o = m;
+    }
+    *reinterpret_cast<float4 *>(rowbuf + g * RMAX + col) =
+        valid ? o : make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < PAIRS; ++p) {
+      const int pair = tid + p * 256;
+      if (pair < R * R) {
+        const int r = pair / R, s2 = pair % R;
+        double acc = 0.0;
+        for (int gi = 0; gi < GROUPS; ++gi)
+          acc += (double)rowbuf[gi * RMAX + r] * (double)rowbuf[gi * RMAX + s2];
+        gacc[p] += acc;
+      }
+    }
+    if (tid < R)
+      for (int gi = 0; gi < GROUPS; ++gi) cmax = fmax(cmax, (double)rowbuf[gi * RMAX + tid]);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int p = 0; p < PAIRS; ++p) {
+    const int pair = tid + p * 256;
+    if (pair < R * R) a.part_gram[(size_t)blockIdx.x * R * R + pair] = gacc[p];
+  }
+  if (tid < R) a.part_max[(size_t)blockIdx.x * R + tid] = cmax;
+}
+
+// Sum the partial Grams; with lam != nullptr also derive lambda (2-norm on the
+// first iteration, max-norm floored at 1 after) and scale G by 1/(l_r l_s).
+__global__ void k_finalize(const double *part_gram, const double *part_max, int nblocks, int R,
+                           double *G, double *lam, const int *iter) {
+  __shared__ double slam[128];
+  const int tid = threadIdx.x;
+  const bool first = (iter == nullptr) || (*iter == 0);
+  for (int r = tid; r < R; r += blockDim.x) {
+    if (lam) {
+      double v;
+      if (first) {
+        double s = 0;
+        for (int b = 0; b < nblocks; ++b) s += part_gram[(size_t)b * R * R + r * R + r];
+        v = sqrt(s);
+      } else {
+        double mx = 0;
+        for (int b = 0; b < nblocks; ++b) mx = fmax(mx, part_max[(size_t)b * R + r]);
+        v = fmax(mx, 1.0);
+      }
+      slam[r] = v;
+      lam[r] = v;
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < R * R; e += blockDim.x) {
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part_gram[(size_t)b * R * R + e];
+    if (lam) s /= slam[e / R] * slam[e % R];
+    G[e] = s;
+  }
+}
+
+// A /= lambda (fp32), bf16 copy, optional partial <A, M> per column.
+template <int LANES>
+__global__ void __launch_bounds__(256) k_scale(float *A, __nv_bfloat16 *Ab, const float *M,
+                                               uint64_t rows, int R, int ldr, const double *lam,
+                                               double *part_inner) {
+  constexpr int GROUPS = 256 / LANES;
+  const int tid = threadIdx.x;
+  const int g = tid / LANES, t = tid % LANES, col = 4 * t;
+  const bool act = col < R;
+  float4 il = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (act) {
+    il.x = col + 0 < R ? (float)(1.0 / lam[col + 0]) : 0.f;
+    il.y = col + 1 < R ? (float)(1.0 / lam[col + 1]) : 0.f;
+    il.z = col + 2 < R ? (float)(1.0 / lam[col + 2]) : 0.f;
+    il.w = col + 3 < R ? (float)(1.0 / lam[col + 3]) : 0.f;
+  }
+  double in0 = 0, in1 = 0, in2 = 0, in3 = 0;
+  for (uint64_t i = (uint64_t)blockIdx.x * GROUPS + g; i < rows; i += (uint64_t)gridDim.x * GROUPS) {
+    if (!act) continue;
+    float4 v = *reinterpret_cast<float4 *>(A + i * ldr + col);
+    v.x *= il.x;
+    v.y *= il.y;
+    v.z *= il.z;
+    v.w *= il.w;
+    *reinterpret_cast<float4 *>(A + i * ldr + col) = v;
+    if (Ab) {
+      __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y);
+      __nv_bfloat162 hi = __floats2bfloat162_rn(v.z, v.w);
+      uint2 raw;
+      raw.x = *reinterpret_cast<uint32_t *>(&lo);
+      raw.y = *reinterpret_cast<uint32_t *>(&hi);
+      *reinterpret_cast<uint2 *>(Ab + i * ldr + col) = raw;
+    }
+    if (part_inner) {
+      const float4 m = *reinterpret_cast<const float4 *>(M + i * ldr + col);
+      in0 += (double)v.x * m.x;
+      in1 += (double)v.y * m.y;
+      in2 += (double)v.z * m.z;
+      in3 += (double)v.w * m.w;
+    }
+  }
+  if (part_inner) {
+    __shared__ double red[256 * 4];
+    red[tid * 4 + 0] = in0;
+    red[tid * 4 + 1] = in1;
+    red[tid * 4 + 2] = in2;
+    red[tid * 4 + 3] = in3;
+    __syncthreads();
+    if (tid < 4 * LANES) {
+      const int tt = tid / 4, c = tid % 4;
+      double s = 0;
+      for (int gi = 0; gi < GROUPS; ++gi) s += red[(gi * LANES + tt) * 4 + c];
+      const int column = 4 * tt + c;
+      if (column < R) part_inner[(size_t)blockIdx.x * R + column] = s;
+    }
+  }
+}
+
+__global__ void k_fit(GramSet g, int nmodes, int R, const double *lam, const double *part_inner,
+                      int nblocks, double *scalars, double *trace, int max_trace, int *iter) {
+  __shared__ double red[256];
+  const int tid = threadIdx.x;
+  double nrm = 0;
+  for (int e = tid; e < R * R; e += blockDim.x) {
+    double h = 1.0;
+    for (int m = 0; m < nmodes; ++m) h *= g.G[m][e];
+    nrm += h * lam[e / R] * lam[e % R];
+  }
+  double inner = 0;
+  for (int r = tid; r < R; r += blockDim.x) {
+    double s = 0;
+    for (int b = 0; b < nblocks; ++b) s += part_inner[(size_t)b * R + r];
+    inner += s * lam[r];
+  }
+  red[tid] = nrm;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (tid < o) red[tid] += red[tid + o];
+    __syncthreads();
+  }
+  const double norm = fabs(red[0]);
+  __syncthreads();
+  red[tid] = inner;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (tid < o) red[tid] += red[tid + o];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const double in = red[0];
+    const double ttn = scalars[0];
+    const double fit = 1.0 - sqrt(ttn + norm - 2.0 * in) / sqrt(ttn);
+    scalars[1] = fit;
+    scalars[2] = norm;
+    scalars[3] = in;
+    const int it = *iter;
+    if (it < max_trace) trace[it] = fit;
+    *iter = it + 1;
+  }
+}
+
+int lanes_for(int R) {
+  if (R <= 16) return 4;
+  if (R <= 32) return 8;
+  if (R <= 64) return 16;
+  if (R <= 128) return 32;
+  throw BadInput("rank above 128 is not supported by the GPU kernels");
+}
+
+template <int LANES>
+constexpr size_t update_smem() {
+  return (size_t)(4 * LANES * 4 * LANES + (256 / LANES) * 4 * LANES) * sizeof(float);
+}
+
+template <int LANES>
+void launch_update(const UpdArgs &u, int nblocks, cudaStream_t s) {
+  k_update<LANES><<<nblocks, 256, update_smem<LANES>(), s>>>(u);
+  ADATM_LAUNCH();
+}
+
+// Kernels with more than 48 KB of dynamic shared memory must be opted in
+// once, before any stream capture.
+void set_attributes() {
+  ADATM_CUDA(cudaFuncSetAttribute(k_update<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)update_smem<4>()));
+  ADATM_CUDA(cudaFuncSetAttribute(k_update<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)update_smem<8>()));
+  ADATM_CUDA(cudaFuncSetAttribute(k_update<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)update_smem<16>()));
+  ADATM_CUDA(cudaFuncSetAttribute(k_update<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)update_smem<32>()));
+  ADATM_CUDA(cudaFuncSetAttribute(k_gram_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  128 * 128 * (int)sizeof(double)));
+}
+
+void run_update(const UpdArgs &u, int nblocks, cudaStream_t s) {
+  switch (lanes_for(u.R)) {
+    case 4: launch_update<4>(u, nblocks, s); break;
+    case 8: launch_update<8>(u, nblocks, s); break;
+    case 16: launch_update<16>(u, nblocks, s); break;
+    default: launch_update<32>(u, nblocks, s); break;
+  }
+}
+
+}  // namespace
+
+void factor_init_device(float *A, __nv_bfloat16 *Ab, uint64_t rows, int R, int ldr, uint64_t seed,
+                        uint64_t mode, cudaStream_t s) {
+  auto hmix = [](uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  const uint64_t key = hmix(seed * 0x100000001B3ull + mode);
+  const uint64_t n = rows * (uint64_t)ldr;
+  if (n == 0) return;
+  k_factor_init<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, Ab, rows, R, ldr, key);
+  ADATM_LAUNCH();
+}
+
+void to_bf16(const float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s) {
+  const uint64_t n = rows * (uint64_t)ldr;
+  if (n == 0) return;
+  k_to_bf16<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, Ab, n);
+  ADATM_LAUNCH();
+}
+
+void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, cudaStream_t s) {
+  UpdArgs u;
+  u.M = A;
+  u.vinv = nullptr;
+  u.A = nullptr;
+  u.rows = rows;
+  u.R = R;
+  u.ldr = ldr;
+  u.part_gram = w.part_gram.get();
+  u.part_max = w.part_max.get();
+  run_update(u, w.nblocks, s);
+  k_finalize<<<1, 256, 0, s>>>(w.part_gram.get(), w.part_max.get(), w.nblocks, R, G, nullptr,
+                               nullptr);
+  ADATM_LAUNCH();
+}
+
+void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s) {
+  const int blocks = 256;
+  DevBuf<double> part(blocks);
+  k_frob_partial<<<blocks, kFrobThreads, 0, s>>>(vals, n, part.get());
+  ADATM_LAUNCH();
+  k_frob_final<<<1, 32, 0, s>>>(part.get(), blocks, w.scalars.get());
+  ADATM_LAUNCH();
+  ADATM_CUDA(cudaStreamSynchronize(s));
+}
+
+void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s) {
+  const size_t smem = (size_t)w.R * w.R * sizeof(double);
+  k_gram_inverse<<<1, 256, smem, s>>>(g, w.nmodes, mode, w.R, w.vinv64.get(), w.vinv32.get());
+  ADATM_LAUNCH();
+}
+
+void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
+                   bool inner, AlsWork &w, cudaStream_t s) {
+  UpdArgs u;
+  u.M = M;
+  u.vinv = w.vinv32.get();
+  u.A = A;
+  u.rows = rows;
+  u.R = w.R;
+  u.ldr = w.ldr;
+  u.part_gram = w.part_gram.get();
+  u.part_max = w.part_max.get();
+  run_update(u, w.nblocks, s);
+  k_finalize<<<1, 256, 0, s>>>(w.part_gram.get(), w.part_max.get(), w.nblocks, w.R, G_mode,
+                               w.lambda.get(), w.iter.get());
+  ADATM_LAUNCH();
+  double *pi = inner ? w.part_inner.get() : nullptr;
+  switch (lanes_for(w.R)) {
+    case 4: k_scale<4><<<w.nblocks, 256, 0, s>>>(A, Ab, M, rows, w.R, w.ldr, w.lambda.get(), pi); break;
+    case 8: k_scale<8><<<w.nblocks, 256, 0, s>>>(A, Ab, M, rows, w.R, w.ldr, w.lambda.get(), pi); break;
+    case 16: k_scale<16><<<w.nblocks, 256, 0, s>>>(A, Ab, M, rows, w.R, w.ldr, w.lambda.get(), pi); break;
+    default: k_scale<32><<<w.nblocks, 256, 0, s>>>(A, Ab, M, rows, w.R, w.ldr, w.lambda.get(), pi); break;
+  }
+  ADATM_LAUNCH();
+}
+
+void fit(const GramSet &g, AlsWork &w, cudaStream_t s) {
+  k_fit<<<1, 256, 0, s>>>(g, w.nmodes, w.R, w.lambda.get(), w.part_inner.get(), w.nblocks,
+                          w.scalars.get(), w.fit_trace.get(), w.max_trace, w.iter.get());
+  ADATM_LAUNCH();
+}
+
+}  // namespace adatm

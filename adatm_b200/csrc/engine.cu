@@ -1,0 +1,305 @@
+// engine.cu -- tensor + plan + trees + memo rows + factors + CP-ALS sweep.
+#include <algorithm>
+#include <cstring>
+
+#include "engine.hpp"
+
+namespace adatm {
+
+namespace {
+int depth_of(const DevCsf &c, int mode) {
+  for (int l = 0; l < c.nmodes; ++l)
+    if ((int)c.dim_perm[l] == mode) return l;
+  throw BadInput("mode missing from the tree's level order");
+}
+}  // namespace
+
+Engine::Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<DevCsf>> trees,
+               uint64_t rank, const Plan &plan, const EngineOptions &opt, cudaStream_t stream)
+    : coo_(std::move(coo)), R_(rank), ldr_(ldr_of(rank)), plan_(plan), opt_(opt),
+      stream_(stream), csf_(std::move(trees)) {
+  const int N = coo_->nmodes;
+  if (rank == 0 || rank > 128) throw BadInput("rank must be 1..128");
+  if (csf_.empty()) {
+    for (int g = 0; g < plan_.n_csf; ++g) {
+      csf_.emplace_back(std::make_shared<DevCsf>());
+      csf_build(*coo_, plan_.grp[g].o_opt, *csf_.back(), stream_);
+    }
+  }
+  if ((int)csf_.size() != plan_.n_csf) throw BadInput("tree count does not match the plan");
+  for (int g = 0; g < plan_.n_csf; ++g) {
+    const Group &gp = plan_.grp[g];
+    for (uint64_t deg = 0; deg < gp.n_imten; ++deg) {
+      const uint64_t lvl = gp.begin_imten - 1 - deg;
+      const size_t n = (size_t)csf_[g]->nfibs[lvl] * ldr_;
+      memo_[g][deg].alloc(n);
+      ADATM_CUDA(cudaMemsetAsync(memo_[g][deg].get(), 0, n * sizeof(float), stream_));
+    }
+  }
+  uint64_t maxdim = 1;
+  for (int m = 0; m < N; ++m) {
+    maxdim = std::max(maxdim, coo_->dims[m]);
+    A_[m].alloc((size_t)coo_->dims[m] * ldr_);
+    ADATM_CUDA(cudaMemsetAsync(A_[m].get(), 0, A_[m].bytes(), stream_));
+    if (opt_.factor_type == FactorType::BF16) {
+      Ab_[m].alloc((size_t)coo_->dims[m] * ldr_);
+      ADATM_CUDA(cudaMemsetAsync(Ab_[m].get(), 0, Ab_[m].bytes(), stream_));
+    }
+    G_[m].alloc((size_t)R_ * R_);
+  }
+  M_.alloc((size_t)maxdim * ldr_);
+  int sms = 148;
+  {
+    int dev = 0;
+    ADATM_CUDA(cudaGetDevice(&dev));
+    ADATM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  w_.init(N, (int)R_, 2 * sms, opt_.max_iters);
+  build_walks();
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+Engine::~Engine() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  if (staging_) cudaFreeHost(staging_);
+}
+
+float *Engine::staging(size_t n) {
+  if (n > staging_n_) {
+    if (staging_) cudaFreeHost(staging_);
+    staging_ = nullptr;
+    staging_n_ = 0;
+    ADATM_CUDA(cudaMallocHost(&staging_, n * sizeof(float)));
+    staging_n_ = n;
+  }
+  return staging_;
+}
+
+size_t Engine::memo_bytes() const {
+  size_t b = 0;
+  for (int g = 0; g < kMaxModes; ++g)
+    for (int d = 0; d < kMaxModes; ++d) b += memo_[g][d].bytes();
+  return b;
+}
+
+size_t Engine::csf_bytes() const {
+  size_t b = 0;
+  for (auto &c : csf_) b += c->device_bytes();
+  return b;
+}
+
+void Engine::build_walks() {
+  const int N = coo_->nmodes;
+  for (int m = 0; m < N; ++m) {
+    const int g = (int)plan_.use_csfs[m];
+    const int tag = (int)plan_.use_tags[m];
+    const DevCsf &c = *csf_[g];
+    const Group &gp = plan_.grp[g];
+    const int d = depth_of(c, m);
+    auto direct = std::make_unique<TreeWalk>();
+    direct->csf = &c;
+    direct->R = (int)R_;
+    direct->ldr = ldr_;
+    direct->src = N - 1;
+    direct->out = d;
+    direct->chunk = opt_.chunk_leaf;
+    walk_prepare(*direct, stream_);
+    auto w = std::make_unique<TreeWalk>();
+    w->csf = &c;
+    w->R = (int)R_;
+    w->ldr = ldr_;
+    w->src = N - 1;
+    w->out = d;
+    w->chunk = opt_.chunk_leaf;
+    if (tag == 0 && gp.n_imten > 0) {
+      // memo root: store level begin_imten-1-deg into memo tree deg
+      for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
+        w->store[gp.begin_imten - 1 - deg] = memo_[g][deg].get();
+    } else if (tag == 1) {
+      // reuse: the leading memo levels that lie below the output level
+      // (mttkrp.c:1578-1588 with rcsf_reverse_mode_order, adatm_rcsf.c:313-326)
+      const uint64_t b = gp.begin_imten;
+      uint64_t rd[kMaxModes + 1] = {0};
+      uint64_t j = 0;
+      for (int64_t i = (int64_t)b; i >= 0; --i)
+        if (i != d) rd[j++] = (uint64_t)i;
+      uint64_t indeg = 0;
+      for (uint64_t i = 0; i < gp.n_imten; ++i)
+        if (b - i == rd[i]) ++indeg;
+      if (indeg > 0) {
+        w->src = (int)(b - indeg);
+        w->src_rows = memo_[g][indeg - 1].get();
+        w->chunk = opt_.chunk_rows;
+      }
+    }
+    walk_prepare(*w, stream_);
+    walk_[m] = std::move(w);
+    direct_[m] = std::move(direct);
+  }
+}
+
+LevelFactors Engine::level_factors(int g) const {
+  LevelFactors f;
+  const DevCsf &c = *csf_[g];
+  for (int l = 0; l < c.nmodes; ++l) {
+    const int m = (int)c.dim_perm[l];
+    f.U[l] = opt_.factor_type == FactorType::BF16 ? (const void *)Ab_[m].get()
+                                                   : (const void *)A_[m].get();
+  }
+  return f;
+}
+
+void Engine::mttkrp(int mode, float *out) {
+  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
+  walk_launch(*walk_[mode], level_factors((int)plan_.use_csfs[mode]), opt_.factor_type, out,
+              stream_);
+}
+
+void Engine::mttkrp_direct(int mode, float *out) {
+  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
+  walk_launch(*direct_[mode], level_factors((int)plan_.use_csfs[mode]), opt_.factor_type, out,
+              stream_);
+}
+
+int Engine::kernels_per_mttkrp(int mode) const {
+  const TreeWalk &w = *walk_[mode];
+  if (w.nchunks == 0) return 0;
+  return w.has_store() ? 2 : 1;
+}
+
+int Engine::kernels_per_sweep() const {
+  int k = 1;  // fit
+  for (int m = 0; m < coo_->nmodes; ++m) k += kernels_per_mttkrp(m) + 4;
+  return k;
+}
+
+double Engine::mttkrp_bytes(int mode) const {
+  const TreeWalk &w = *walk_[mode];
+  uint64_t dl[kMaxModes] = {0};
+  for (int l = 0; l < w.csf->nmodes; ++l) dl[l] = coo_->dims[w.csf->dim_perm[l]];
+  return walk_compulsory_bytes(w, opt_.factor_type, dl, coo_->dims[mode]);
+}
+
+void Engine::init_factors(uint64_t seed) {
+  for (int m = 0; m < coo_->nmodes; ++m)
+    factor_init_device(A_[m].get(), Ab_[m].get(), coo_->dims[m], (int)R_, ldr_, seed, (uint64_t)m,
+                       stream_);
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::set_factors(const double *const *host) {
+  size_t total = 0;
+  for (int m = 0; m < coo_->nmodes; ++m) total += (size_t)coo_->dims[m] * ldr_;
+  float *buf = staging(total);
+  size_t off = 0;
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    const uint64_t I = coo_->dims[m];
+    float *b = buf + off;
+    for (uint64_t i = 0; i < I; ++i) {
+      for (uint64_t r = 0; r < R_; ++r) b[i * ldr_ + r] = (float)host[m][i * R_ + r];
+      for (uint64_t r = R_; r < (uint64_t)ldr_; ++r) b[i * ldr_ + r] = 0.f;
+    }
+    ADATM_CUDA(cudaMemcpyAsync(A_[m].get(), b, (size_t)I * ldr_ * sizeof(float),
+                               cudaMemcpyHostToDevice, stream_));
+    if (Ab_[m].get()) to_bf16(A_[m].get(), Ab_[m].get(), I, ldr_, stream_);
+    off += (size_t)I * ldr_;
+  }
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::get_factors(double *const *host) {
+  size_t total = 0;
+  for (int m = 0; m < coo_->nmodes; ++m) total += (size_t)coo_->dims[m] * ldr_;
+  float *buf = staging(total);
+  size_t off = 0;
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    ADATM_CUDA(cudaMemcpyAsync(buf + off, A_[m].get(), (size_t)coo_->dims[m] * ldr_ * sizeof(float),
+                               cudaMemcpyDeviceToHost, stream_));
+    off += (size_t)coo_->dims[m] * ldr_;
+  }
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  off = 0;
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    const uint64_t I = coo_->dims[m];
+    for (uint64_t i = 0; i < I; ++i)
+      for (uint64_t r = 0; r < R_; ++r) host[m][i * R_ + r] = (double)buf[off + i * ldr_ + r];
+    off += (size_t)I * ldr_;
+  }
+}
+
+void Engine::get_lambda(double *host) const {
+  ADATM_CUDA(cudaMemcpyAsync(host, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::als_begin() {
+  for (int m = 0; m < coo_->nmodes; ++m)
+    gram(A_[m].get(), coo_->dims[m], (int)R_, ldr_, G_[m].get(), w_, stream_);
+  frob_sq(csf_[0]->vals64.get(), coo_->nnz, w_, stream_);
+  ADATM_CUDA(cudaMemsetAsync(w_.iter.get(), 0, sizeof(int), stream_));
+  ADATM_CUDA(cudaMemsetAsync(w_.fit_trace.get(), 0, w_.max_trace * sizeof(double), stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::sweep_eager() {
+  const int N = coo_->nmodes;
+  GramSet gs;
+  for (int m = 0; m < kMaxModes; ++m) gs.G[m] = m < N ? G_[m].get() : nullptr;
+  for (int m = 0; m < N; ++m) {
+    mttkrp(m, M_.get());
+    gram_inverse(gs, m, w_, stream_);
+    update_factor(M_.get(), coo_->dims[m], A_[m].get(), Ab_[m].get(), G_[m].get(), m == N - 1, w_,
+                  stream_);
+  }
+  fit(gs, w_, stream_);
+}
+
+void Engine::capture_graph() {
+  if (graph_exec_) return;
+  // kernels set their shared-memory attributes on first use: run the
+  // attribute paths once outside the capture on scratch state
+  ADATM_CUDA(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+  try {
+    sweep_eager();
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(stream_, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  ADATM_CUDA(cudaStreamEndCapture(stream_, &graph_));
+  ADATM_CUDA(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+}
+
+void Engine::sweep() {
+  if (graph_exec_)
+    ADATM_CUDA(cudaGraphLaunch(graph_exec_, stream_));
+  else
+    sweep_eager();
+}
+
+double Engine::fit_host() {
+  double f = 0;
+  ADATM_CUDA(cudaMemcpyAsync(&f, w_.scalars.get() + 1, sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  return f;
+}
+
+int Engine::iter_host() {
+  int it = 0;
+  ADATM_CUDA(cudaMemcpyAsync(&it, w_.iter.get(), sizeof(int), cudaMemcpyDeviceToHost, stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  return it;
+}
+
+void Engine::fit_trace(double *host, int n) {
+  n = std::min(n, w_.max_trace);
+  ADATM_CUDA(cudaMemcpyAsync(host, w_.fit_trace.get(), n * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+}  // namespace adatm

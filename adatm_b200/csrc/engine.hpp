@@ -1,0 +1,102 @@
+// engine.hpp -- one tensor resident in HBM with its plan, CSF trees, memo
+// rows, factor matrices and the CP-ALS sweep.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "als.cuh"
+#include "mttkrp.cuh"
+#include "planner.hpp"
+
+namespace adatm {
+
+struct EngineOptions {
+  FactorType factor_type = FactorType::F32;
+  uint32_t chunk_leaf = 32;   // source units per chunk, nonzero sources
+  uint32_t chunk_rows = 16;   // source units per chunk, memo-row sources
+  int max_iters = 1024;       // capacity of the device fit trace
+};
+
+class Engine {
+ public:
+  // trees: prebuilt CSF trees of the plan (empty = build them here)
+  Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<DevCsf>> trees,
+         uint64_t rank, const Plan &plan, const EngineOptions &opt, cudaStream_t stream);
+  ~Engine();
+  Engine(const Engine &) = delete;
+  Engine &operator=(const Engine &) = delete;
+
+  int nmodes() const { return coo_->nmodes; }
+  uint64_t rank() const { return R_; }
+  int ldr() const { return ldr_; }
+  uint64_t nnz() const { return coo_->nnz; }
+  const uint64_t *dims() const { return coo_->dims; }
+  const Plan &plan() const { return plan_; }
+  const DevCsf &csf(int g) const { return *csf_[g]; }
+  int n_csf() const { return (int)csf_.size(); }
+  const DevCoo &coo() const { return *coo_; }
+  const std::vector<std::shared_ptr<DevCsf>> &trees() const { return csf_; }
+  int kernels_per_mttkrp(int mode) const;
+  int kernels_per_sweep() const;
+  cudaStream_t stream() const { return stream_; }
+  FactorType factor_type() const { return opt_.factor_type; }
+  const TreeWalk &walk(int mode) const { return *walk_[mode]; }
+  size_t memo_bytes() const;
+  size_t csf_bytes() const;
+
+  // factors
+  void init_factors(uint64_t seed);
+  void set_factors(const double *const *host);          // dims[m] x R each
+  void get_factors(double *const *host);
+  void get_lambda(double *host) const;
+  float *factor(int m) { return A_[m].get(); }
+
+  // MTTKRP of `mode` following the plan (tags 0/1/2) into out (dims x ldr,
+  // zeroed here). Memo reuse (tag 1) expects the group's memo root to have
+  // run on the current factors of the memoized levels.
+  void mttkrp(int mode, float *out);
+  // MTTKRP of `mode` recomputed on its group's tree without memo rows.
+  void mttkrp_direct(int mode, float *out);
+  float *mttkrp_buffer() { return M_.get(); }
+  const float *memo_rows(int g, int deg) const { return memo_[g][deg].get(); }
+
+  // CP-ALS
+  void als_begin();                      // Grams, ||X||^2, iteration counter
+  void sweep();                          // one ALS iteration (graph replay if captured)
+  void sweep_eager();                    // one ALS iteration, plain launches
+  void capture_graph();
+  double fit_host();                     // last fit (synchronises)
+  int iter_host();
+  void fit_trace(double *host, int n);
+
+  // compulsory HBM bytes of the MTTKRP of `mode` (roofline numerator)
+  double mttkrp_bytes(int mode) const;
+
+ private:
+  void build_walks();
+  LevelFactors level_factors(int g) const;
+
+  std::shared_ptr<const DevCoo> coo_;
+  uint64_t R_;
+  int ldr_;
+  Plan plan_;
+  EngineOptions opt_;
+  cudaStream_t stream_;
+  std::vector<std::shared_ptr<DevCsf>> csf_;
+  DevBuf<float> memo_[kMaxModes][kMaxModes];
+  std::unique_ptr<TreeWalk> walk_[kMaxModes];
+  std::unique_ptr<TreeWalk> direct_[kMaxModes];
+  DevBuf<float> A_[kMaxModes];
+  DevBuf<__nv_bfloat16> Ab_[kMaxModes];
+  DevBuf<double> G_[kMaxModes];
+  DevBuf<float> M_;
+  AlsWork w_;
+  float *staging_ = nullptr;     // pinned host rows for factor transfers
+  size_t staging_n_ = 0;
+  float *staging(size_t n);
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+};
+
+}  // namespace adatm

@@ -1,0 +1,72 @@
+// mttkrp.cuh -- the MTTKRP kernels on CSF trees and their launch plans.
+//
+// Every MTTKRP of the reference (plain root / internal / leaf, memo root,
+// memo reuse; mttkrp.c:241-1682) is one of two tree walks over a source
+// level S and an output level d of one CSF tree:
+//
+//  * contract (S > d): every unit of level S (a nonzero when S = N-1, else a
+//    stored memo row T_S) is multiplied by its factor row and summed into its
+//    level S-1 parent; a completed node of level l > d multiplies its sum by
+//    its own factor row and adds it to its parent; a completed node of level
+//    d is written to the output row fids[d][node], multiplied by the prefix
+//    product P_{d-1} of the factor rows on its root path (d > 0). Completed
+//    nodes of the levels listed in `store` are also written to memo rows.
+//  * scatter (S == d): every unit u adds src(u) * P_{d-1} to output row
+//    fids[d][u] (leaf MTTKRP when d = N-1, memo reuse at its stored level).
+//
+// Work is split into chunks of `chunk` consecutive source units, one chunk
+// per row group of LANES lanes (each lane holds 4 of the R columns), so the
+// split follows nonzeros, not root slices (the reference's omp
+// schedule(dynamic,16) over slices, mttkrp.c:392, cannot balance a slice
+// holding 16% of the nonzeros). Nodes cut by a chunk boundary are combined
+// with vector atomics; for memo rows those nodes are zeroed first by a
+// separate launch, all other memo rows are written exactly once.
+#pragma once
+
+#include "csf_build.cuh"
+
+namespace adatm {
+
+enum class FactorType : int { F32 = 0, BF16 = 1 };
+
+// Factor row matrices of one tree, in level order (U[l] belongs to mode
+// dim_perm[l]); fp32 or bf16 with leading dimension ldr.
+struct LevelFactors {
+  const void *U[kMaxModes] = {nullptr};
+};
+
+struct TreeWalk {
+  int nmodes = 0;
+  int src = 0;                 // source level S
+  int out = 0;                 // output level d
+  int R = 0, ldr = 0;
+  uint32_t chunk = 32;
+  uint32_t nchunks = 0;
+  uint64_t nunits = 0;         // nodes of level S
+  const DevCsf *csf = nullptr;
+  const float *src_rows = nullptr;           // memo rows of level S (S < N-1)
+  float *store[kMaxModes] = {nullptr};       // memo rows written, per level
+  DevBuf<uint32_t> sched;                    // nchunks x (S + 1)
+  bool has_store() const {
+    for (int l = 0; l < kMaxModes; ++l)
+      if (store[l]) return true;
+    return false;
+  }
+};
+
+// Fill the chunk schedule: node ids at levels 0..S-1 of every chunk's first
+// unit, plus a bit mask of the levels whose node began before the chunk.
+void walk_prepare(TreeWalk &w, cudaStream_t s);
+
+// Launch the walk: output rows must be zero beforehand (the caller clears
+// them); memo rows cut by chunk boundaries are zeroed here.
+void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float *out,
+                 cudaStream_t s);
+
+// Bytes the walk must move through HBM (structure read once, memo rows read
+// or written once, factors read once, output written once): the compulsory
+// traffic used for the roofline figure.
+double walk_compulsory_bytes(const TreeWalk &w, FactorType ft, const uint64_t *dims_of_level,
+                             uint64_t out_rows);
+
+}  // namespace adatm

@@ -1,0 +1,260 @@
+/*
+ * adatm_b200.h -- AdaTM's own entry points (the memoized MTTKRP sequence,
+ * its planner and the adaptive CP-ALS) plus the B200 device-resident API.
+ *
+ * Part 1 keeps the names and argument meaning of the reference's internal
+ * headers (src/adatm_rcsf.h, src/adatm_bench.h, src/mttkrp.h,
+ * src/adatm_cpd.h), which the reference's CLI and bench call; the SPLATT
+ * internal types they take (sptensor_t, matrix_t, thd_info, rank_info,
+ * bench_opts) are declared here with the fields those entry points read.
+ * Thread scratch (thd_info) and MPI rank info are accepted and ignored.
+ *
+ * Part 2 is the device-resident interface the B200 build adds: a tensor and
+ * an engine (plan, trees, memo rows, factors) stay in HBM across calls, so
+ * benchmarks and services avoid host copies per MTTKRP.
+ *
+ * Every function returns SPLATT_SUCCESS (1) on success and a
+ * splatt_error_type, or ADATM_ERROR_CUDA for a CUDA runtime failure, with a
+ * message available from adatm_last_error().
+ */
+#ifndef ADATM_B200_H
+#define ADATM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "splatt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ADATM_ERROR_CUDA 4
+
+/* ======================================================================== */
+/* Part 1: SPLATT internal types and the reference's AdaTM entry points     */
+/* ======================================================================== */
+
+typedef splatt_idx_t idx_t;
+typedef splatt_val_t val_t;
+
+typedef struct {
+  idx_t nnz;
+  idx_t nmodes;
+  idx_t *dims;
+  idx_t **ind;
+  val_t *vals;
+  int tiled;
+  int type;
+} sptensor_t;
+
+typedef struct {
+  idx_t I;
+  idx_t J;
+  val_t *vals;
+  int rowmajor;
+} matrix_t;
+
+typedef struct thd_info thd_info;   /* unused by the GPU path; pass NULL */
+typedef struct { int rank; } rank_info;
+
+typedef struct {
+  idx_t niters;
+  idx_t *threads;
+  idx_t nruns;
+  int write;
+  int tile;
+  void *perm;
+} bench_opts;
+
+/* decide_product_order (reference src/adatm_bench.h:33): product_order[m] has
+ * 2*N entries, 1 where MTTKRP m reads factor k unchanged (k < N) or updated
+ * (N + k). */
+void decide_product_order(sptensor_t *const tt, idx_t **product_order);
+
+/* decide_parameters_auto (reference src/adatm_bench.h:46-51): candidate
+ * plans, fiber counts on the GPU, SLIMIT filter, strategy 1 = fewest
+ * predicted products, 2 = least predicted space. Returns n_grp; *grp_prop is
+ * malloc'd (free o_opt of every group, then the array). */
+idx_t decide_parameters_auto(sptensor_t *const tt, idx_t const nfactors, int strategy,
+                             idx_t const **product_order, group_properties **grp_prop);
+
+/* decide_candidate_configs / predict_candidates_adaptive /
+ * limit_candidates_by_space / choose_candidates_by_strategy (reference
+ * src/adatm_bench.h:59-110). */
+idx_t decide_candidate_configs(sptensor_t *const tt, idx_t const **product_order,
+                               configurations_adaptive **configs);
+void predict_candidates_adaptive(sptensor_t *const tt, idx_t const nfactors,
+                                 configurations_adaptive *configs, idx_t const nconfigs);
+idx_t limit_candidates_by_space(configurations_adaptive const *const configs,
+                                idx_t const nconfigs, idx_t **const real_config_locs);
+idx_t choose_candidates_by_strategy(configurations_adaptive const *const configs,
+                                    idx_t const nconfigs, idx_t const *const real_config_locs,
+                                    idx_t const n_real_configs, int strategy);
+
+/* csf_alloc_adaptive (reference src/adatm_rcsf.h:18-23): one tree per
+ * group, built on the GPU; the returned host arrays follow the reference
+ * layout and the device copies stay resident until splatt_free_csf. */
+splatt_csf *csf_alloc_adaptive(sptensor_t *const tt, group_properties *const grp_prop,
+                               idx_t const n_grp, double const *const opts, idx_t *n_csf);
+
+/* rcsf_alloc_adaptive (reference src/adatm_rcsf.h:142-149): memo trees that
+ * alias the CSF fptr/fids arrays and own nfibs*nfactors values each. Their
+ * device rows live in HBM; adatm_rcsf_pull copies them into the host vals. */
+rcsf_seq_adaptive *rcsf_alloc_adaptive(splatt_csf *const ct, idx_t const nfactors,
+                                       group_properties *const grp_prop, idx_t const n_grp,
+                                       idx_t const n_csf, double const *const opts,
+                                       idx_t *n_rcsf);
+
+size_t csf_storage_adaptive(splatt_csf const *const tensors, idx_t const n_csf,
+                            group_properties *const grp_prop, int const n_grp);
+size_t rcsf_storage_adaptive(rcsf_seq_adaptive const *const seq_rcsf, idx_t const n_csf);
+
+/* decide_use_csfs (reference src/mttkrp.h:42-48): tag 0 memo root, 1 memo
+ * reuse, 2 recompute. */
+void decide_use_csfs(idx_t const nmodes, group_properties *const grp_prop, int const n_grp,
+                     idx_t const n_csf, idx_t *use_csfs, idx_t *use_tags);
+
+/* mttkrp_csf_adaptive (reference src/mttkrp.h:51-62): MTTKRP of `mode` into
+ * mats[SPLATT_MAX_NMODES] (host, dims[mode] x J), reading mats[0..N-1]. */
+void mttkrp_csf_adaptive(splatt_csf const *const tensors, rcsf_seq_adaptive const *const rs_seq,
+                         idx_t const n_csf, matrix_t **mats, idx_t const mode,
+                         thd_info *const thds, group_properties *const grp_prop,
+                         int const n_grp, idx_t const use_csf, idx_t const use_tag,
+                         double const *const opts);
+
+/* splatt_cpd_als_adaptive (reference src/adatm_cpd.c:205-215) and
+ * cpd_als_iterate_adaptive (reference src/adatm_cpd.h:29-41). */
+int splatt_cpd_als_adaptive(splatt_csf const *const tensors, rcsf_seq_adaptive *const rs_seq,
+                            splatt_idx_t const n_csf, group_properties const *const grp_prop,
+                            splatt_idx_t const n_grp, splatt_idx_t const *const use_csfs,
+                            splatt_idx_t const *const use_tags, splatt_idx_t const nfactors,
+                            double const *const options, splatt_kruskal *factored);
+double cpd_als_iterate_adaptive(splatt_csf const *const tensors, rcsf_seq_adaptive *const rs_seq,
+                                splatt_idx_t const n_csf, group_properties const *const grp_prop,
+                                splatt_idx_t const n_grp, splatt_idx_t const *const use_csfs,
+                                splatt_idx_t const *const use_tags, matrix_t **mats,
+                                val_t *const lambda, idx_t const nfactors,
+                                rank_info *const rinfo, double const *const opts);
+
+/* bench_adaptm (reference src/adatm_bench.h:22-25): plan, build, then time
+ * opts->niters MTTKRP sequences and print per-mode seconds. */
+void bench_adaptm(sptensor_t *const tt, matrix_t **mats, bench_opts const *const opts);
+
+/* Copy the device memo rows of rs_seq (all sequences, all trees) into their
+ * host vals arrays. Not in the reference, whose memo rows live on the host. */
+int adatm_rcsf_pull(rcsf_seq_adaptive *rs_seq, idx_t n_rcsf);
+
+/* Number of trees in a splatt_csf array returned by this library (for
+ * CSF_ALLOC values whose count the caller cannot infer). */
+int adatm_csf_tree_count(splatt_csf const *tensors, int *n);
+
+/* Free a group_properties array returned by decide_parameters_auto. */
+void adatm_free_groups(group_properties *grp_prop, idx_t n_grp);
+
+/* ======================================================================== */
+/* Part 2: device-resident B200 interface                                   */
+/* ======================================================================== */
+
+typedef struct adatm_tensor adatm_tensor;
+typedef struct adatm_engine adatm_engine;
+
+/* A memoization plan in flat form. */
+typedef struct adatm_plan {
+  int nmodes;
+  int n_grp;
+  uint64_t memo_mode[8];
+  uint64_t begin_imten[8];
+  uint64_t n_imten[8];
+  uint64_t o_opt[8][8];
+  uint64_t use_csfs[8];
+  uint64_t use_tags[8];
+} adatm_plan;
+
+typedef struct adatm_candidate {
+  adatm_plan plan;
+  uint64_t pspace;
+  uint64_t pops;
+} adatm_candidate;
+
+const char *adatm_last_error(void);
+
+/* Select the CUDA device for the calling thread (the library carries its own
+ * CUDA runtime, so a framework's device selection does not reach it). */
+int adatm_set_device(int device);
+
+/* COO tensor into HBM. With clean != 0, duplicates are summed in input order
+ * and empty slices of every mode are compacted (dims shrink accordingly). */
+int adatm_tensor_from_coo(int nmodes, uint64_t nnz, const uint64_t *dims,
+                          const uint64_t *const *inds, const double *vals, int clean,
+                          adatm_tensor **out);
+/* Seeded synthetic tensor, generated and cleaned on the GPU: mode m's
+ * indices are uniform (alpha[m] <= 0) or Zipf(alpha[m]) with P(k) ~ (k+1)^-a;
+ * values uniform(0,1) (value_kind 0) or lognormal(mu, sigma) (value_kind 1). */
+int adatm_tensor_generate(int nmodes, const uint64_t *dims, uint64_t nnz, const double *alpha,
+                          int value_kind, double mu, double sigma, uint64_t seed,
+                          adatm_tensor **out);
+int adatm_tensor_info(const adatm_tensor *t, int *nmodes, uint64_t *nnz, uint64_t *dims);
+/* inds: nmodes x nnz (mode-major), vals: nnz */
+int adatm_tensor_download(const adatm_tensor *t, uint64_t *inds, double *vals);
+void adatm_tensor_free(adatm_tensor *t);
+
+/* Fiber counts per level of the tree in level order `perm` (count_nfibs). */
+int adatm_tensor_count_nfibs(const adatm_tensor *t, const uint64_t *perm, uint64_t *nfibs);
+
+/* Analytic plan (decide_parameters_auto); cands (may be NULL) receives up to
+ * max_cands candidates with their predictions, *ncands their number, *chosen
+ * the reference's returned position. */
+int adatm_plan_analytic(const adatm_tensor *t, uint64_t rank, int strategy, adatm_plan *out,
+                        adatm_candidate *cands, int max_cands, int *ncands, int *chosen);
+/* SPLATT's plain allocations (csf_alloc = SPLATT_CSF_ONEMODE/TWOMODE/ALLMODE). */
+int adatm_plan_splatt(const adatm_tensor *t, int csf_alloc, adatm_plan *out);
+
+/* Engine: trees, memo rows and factors for one plan and rank.
+ * factor_bf16 != 0 keeps a BF16 copy of every factor for the gathers
+ * (accumulation stays FP32). chunk_leaf/chunk_rows: source units per chunk
+ * (0 = defaults). The engine copies what it needs from the tensor. */
+int adatm_engine_create(const adatm_tensor *t, uint64_t rank, const adatm_plan *plan,
+                        int factor_bf16, uint32_t chunk_leaf, uint32_t chunk_rows,
+                        adatm_engine **out);
+void adatm_engine_free(adatm_engine *e);
+int adatm_engine_csf_count(const adatm_engine *e, int *n_csf);
+int adatm_engine_csf_shape(const adatm_engine *e, int g, uint64_t *nfibs, uint64_t *dim_perm);
+/* Host copies of tree g in the reference layout: fptr[l] (nfibs[l]+1),
+ * fids[l] (nfibs[l], fids[0] = root ids), vals (nnz, FP64). */
+int adatm_engine_csf_arrays(const adatm_engine *e, int g, uint64_t *const *fptr,
+                            uint64_t *const *fids, double *vals);
+int adatm_engine_memory(const adatm_engine *e, uint64_t *csf_bytes, uint64_t *memo_bytes);
+
+int adatm_engine_init_factors(adatm_engine *e, uint64_t seed);
+int adatm_engine_set_factors(adatm_engine *e, const double *const *mats);
+int adatm_engine_get_factors(adatm_engine *e, double *const *mats, double *lambda);
+
+/* MTTKRP of `mode` by the plan (memo root / reuse / recompute) or directly on
+ * the mode's tree without memo rows; out: dims[mode] x rank, host FP64. */
+int adatm_engine_mttkrp(adatm_engine *e, uint64_t mode, double *out);
+int adatm_engine_mttkrp_direct(adatm_engine *e, uint64_t mode, double *out);
+/* Memo rows of group g, tree deg, as host FP64 (nfibs[level] x rank). */
+int adatm_engine_memo(adatm_engine *e, int g, int deg, double *out);
+
+/* CP-ALS: Grams and ||X||^2, then up to niters sweeps, stopping when
+ * |fit - previous| < tol after the first; use_graph captures one sweep in a
+ * CUDA graph. trace (may be NULL) receives one fit per sweep. */
+int adatm_engine_als(adatm_engine *e, uint64_t niters, double tol, int use_graph, double *fit,
+                     uint64_t *iters, double *trace);
+int adatm_engine_als_begin(adatm_engine *e, int use_graph);
+/* Time `count` sweeps (or MTTKRPs of `mode`) on the engine's stream with CUDA
+ * events; *ms is the total. */
+int adatm_engine_time_sweeps(adatm_engine *e, int count, float *ms);
+int adatm_engine_time_mttkrp(adatm_engine *e, uint64_t mode, int count, float *ms);
+int adatm_engine_fit(adatm_engine *e, double *fit);
+/* Compulsory HBM bytes of the MTTKRP of `mode`. */
+int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
+/* Number of kernel launches of one sweep and of one MTTKRP of `mode`. */
+int adatm_engine_launch_counts(adatm_engine *e, uint64_t mode, int *per_sweep, int *per_mttkrp);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
