@@ -21,15 +21,27 @@ def main():
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--bf16", action="store_true")
     ap.add_argument("--plain", action="store_true")
+    ap.add_argument("--time", action="store_true", help="print per-mode MTTKRP and sweep times")
+    ap.add_argument("--chunk", type=int, default=0, help="source units per chunk (0 = default)")
     a = ap.parse_args()
     dims = [int(x) for x in a.dims.split(",")]
     A.lib().adatm_set_device(0)
     t = A.Tensor.generate(dims, a.nnz, alpha=a.alpha, seed=0)
     plan = A.plan_splatt(t, A.CSF_ALLMODE) if a.plain else A.plan_analytic(t, a.rank)[0]
-    e = A.Engine(t, a.rank, plan, bf16=a.bf16)
+    e = A.Engine(t, a.rank, plan, bf16=a.bf16, chunk_leaf=a.chunk, chunk_rows=a.chunk)
     e.init_factors(0)
     res = e.als(a.sweeps, 0.0, graph=False)
-    print(f"nnz {t.info()[1]} plan {plan['groups']} fit {res['fit']:.6f}")
+    print(f"nnz {t.info()[1]} plan {plan['groups']} fit {res['fit']:.6f} trace {res['trace']}")
+    if a.time:
+        n = len(dims)
+        for m in range(n):
+            e.time_mttkrp(m, 3)
+            ms = e.time_mttkrp(m, 20) / 20
+            gbs = e.mttkrp_bytes(m) / (ms * 1e-3) / 1e9
+            print(f"mode {m} tag {plan['use_tags'][m]}: {ms * 1e3:8.1f} us  {gbs:7.1f} GB/s compulsory")
+        e.als_begin(graph=True)
+        e.time_sweeps(3)
+        print(f"sweep (graph): {e.time_sweeps(50) / 50:.3f} ms")
 
 
 if __name__ == "__main__":
