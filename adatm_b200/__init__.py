@@ -572,3 +572,9 @@ class Engine:
         b = C.c_int(0)
         _check(lib().adatm_engine_launch_counts(self._h, mode, C.byref(a), C.byref(b)), "launch_counts")
         return a.value, b.value
+
+
+def gram_device(A_ptr, rows, R, ldr, G_ptr):
+    """G = A^T A (FP64) for a device row matrix; pointers are device addresses
+    (e.g. torch tensor .data_ptr())."""
+    _check(lib().adatm_gram(C.c_void_p(A_ptr), rows, R, ldr, C.c_void_p(G_ptr)), "adatm_gram")

@@ -1120,7 +1120,7 @@ int adatm_engine_time_mttkrp(adatm_engine *e, uint64_t mode, int count, float *m
     ADATM_CUDA(cudaEventCreate(&b));
     ADATM_CUDA(cudaStreamSynchronize(g.stream()));
     ADATM_CUDA(cudaEventRecord(a, g.stream()));
-    for (int i = 0; i < count; ++i) g.mttkrp((int)mode, g.mttkrp_buffer());
+    for (int i = 0; i < count; ++i) g.mttkrp_as((int)mode, g.mttkrp_buffer(), g.sweep_type((int)mode));
     ADATM_CUDA(cudaEventRecord(b, g.stream()));
     ADATM_CUDA(cudaEventSynchronize(b));
     ADATM_CUDA(cudaEventElapsedTime(ms, a, b));
@@ -1137,6 +1137,22 @@ int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes) {
   return guarded([&] {
     if (mode >= (uint64_t)e->eng->nmodes()) throw BadInput("mode out of range");
     *bytes = e->eng->mttkrp_bytes((int)mode);
+  });
+}
+
+int adatm_gram(const float *A, uint64_t rows, int R, int ldr, double *G) {
+  return guarded([&] {
+    if (R < 1 || R > 128 || ldr < R || ldr % 4 != 0) throw BadInput("adatm_gram: bad R or ldr");
+    if (((uintptr_t)A & 15) != 0) throw BadInput("adatm_gram: A must be 16-byte aligned");
+    StreamOwner s;
+    int dev = 0, sms = 148;
+    ADATM_CUDA(cudaGetDevice(&dev));
+    ADATM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    AlsWork w;
+    w.init(1, R, 2 * sms, 1);
+    w.ldr = ldr;
+    gram(A, rows, R, ldr, G, w, s.s);
+    ADATM_CUDA(cudaStreamSynchronize(s.s));
   });
 }
 

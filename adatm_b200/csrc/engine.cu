@@ -139,27 +139,39 @@ void Engine::build_walks() {
   }
 }
 
-LevelFactors Engine::level_factors(int g) const {
+LevelFactors Engine::level_factors(int g, FactorType ft) const {
   LevelFactors f;
   const DevCsf &c = *csf_[g];
   for (int l = 0; l < c.nmodes; ++l) {
     const int m = (int)c.dim_perm[l];
-    f.U[l] = opt_.factor_type == FactorType::BF16 ? (const void *)Ab_[m].get()
-                                                   : (const void *)A_[m].get();
+    f.U[l] = ft == FactorType::BF16 ? (const void *)Ab_[m].get() : (const void *)A_[m].get();
   }
   return f;
 }
 
-void Engine::mttkrp(int mode, float *out) {
+void Engine::mttkrp_as(int mode, float *out, FactorType ft) {
   ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
-  walk_launch(*walk_[mode], level_factors((int)plan_.use_csfs[mode]), opt_.factor_type, out,
-              stream_);
+  walk_launch(*walk_[mode], level_factors((int)plan_.use_csfs[mode], ft), ft, out, stream_);
+}
+
+void Engine::mttkrp(int mode, float *out) { mttkrp_as(mode, out, opt_.factor_type); }
+
+FactorType Engine::sweep_type(int mode) const {
+  // The last mode's MTTKRP M also gives <X, Z> for the fit. An error E in M
+  // moves the computed residual by -2<E, M V^-1>, a positive-definite term
+  // that BF16 gathers make as large as the residual itself (the fit then
+  // overshoots, or its square root goes negative). So every MTTKRP of the
+  // tree that feeds the last mode -- its own walk and the memo rows it
+  // reuses -- reads FP32 rows.
+  const int N = coo_->nmodes;
+  if (opt_.factor_type == FactorType::F32) return FactorType::F32;
+  return plan_.use_csfs[mode] == plan_.use_csfs[N - 1] ? FactorType::F32 : opt_.factor_type;
 }
 
 void Engine::mttkrp_direct(int mode, float *out) {
   ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
-  walk_launch(*direct_[mode], level_factors((int)plan_.use_csfs[mode]), opt_.factor_type, out,
-              stream_);
+  walk_launch(*direct_[mode], level_factors((int)plan_.use_csfs[mode], opt_.factor_type),
+              opt_.factor_type, out, stream_);
 }
 
 int Engine::kernels_per_mttkrp(int mode) const {
@@ -178,7 +190,7 @@ double Engine::mttkrp_bytes(int mode) const {
   const TreeWalk &w = *walk_[mode];
   uint64_t dl[kMaxModes] = {0};
   for (int l = 0; l < w.csf->nmodes; ++l) dl[l] = coo_->dims[w.csf->dim_perm[l]];
-  return walk_compulsory_bytes(w, opt_.factor_type, dl, coo_->dims[mode]);
+  return walk_compulsory_bytes(w, sweep_type(mode), dl, coo_->dims[mode]);
 }
 
 void Engine::init_factors(uint64_t seed) {
@@ -248,7 +260,7 @@ void Engine::sweep_eager() {
   GramSet gs;
   for (int m = 0; m < kMaxModes; ++m) gs.G[m] = m < N ? G_[m].get() : nullptr;
   for (int m = 0; m < N; ++m) {
-    mttkrp(m, M_.get());
+    mttkrp_as(m, M_.get(), sweep_type(m));
     gram_inverse(gs, m, w_, stream_);
     update_factor(M_.get(), coo_->dims[m], A_[m].get(), Ab_[m].get(), G_[m].get(), m == N - 1, w_,
                   stream_);

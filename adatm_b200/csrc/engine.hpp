@@ -56,6 +56,10 @@ class Engine {
   // zeroed here). Memo reuse (tag 1) expects the group's memo root to have
   // run on the current factors of the memoized levels.
   void mttkrp(int mode, float *out);
+  // same, with the factor rows read in the given precision
+  void mttkrp_as(int mode, float *out, FactorType ft);
+  // Row type of mode `mode`'s MTTKRP inside a sweep.
+  FactorType sweep_type(int mode) const;
   // MTTKRP of `mode` recomputed on its group's tree without memo rows.
   void mttkrp_direct(int mode, float *out);
   float *mttkrp_buffer() { return M_.get(); }
@@ -75,7 +79,7 @@ class Engine {
 
  private:
   void build_walks();
-  LevelFactors level_factors(int g) const;
+  LevelFactors level_factors(int g, FactorType ft) const;
 
   std::shared_ptr<const DevCoo> coo_;
   uint64_t R_;

@@ -94,6 +94,7 @@ struct GroupMeta {
   float v[kBatch];
   uint32_t wfid[kBatch];
   uint32_t wend[kBatch];
+  uint32_t pad;  // 132-byte stride: the groups of a warp start on different banks
 };
 
 template <int LANES>

@@ -243,13 +243,22 @@ int adatm_engine_memo(adatm_engine *e, int g, int deg, double *out);
 int adatm_engine_als(adatm_engine *e, uint64_t niters, double tol, int use_graph, double *fit,
                      uint64_t *iters, double *trace);
 int adatm_engine_als_begin(adatm_engine *e, int use_graph);
-/* Time `count` sweeps (or MTTKRPs of `mode`) on the engine's stream with CUDA
- * events; *ms is the total. */
+/* Time `count` sweeps (or MTTKRPs of `mode`, with the row type the sweep
+ * uses for that mode) on the engine's stream with CUDA events; *ms is the
+ * total. */
 int adatm_engine_time_sweeps(adatm_engine *e, int count, float *ms);
 int adatm_engine_time_mttkrp(adatm_engine *e, uint64_t mode, int count, float *ms);
 int adatm_engine_fit(adatm_engine *e, double *fit);
-/* Compulsory HBM bytes of the MTTKRP of `mode`. */
+/* Compulsory HBM bytes of the MTTKRP of `mode` as a sweep runs it. With BF16
+ * rows, the tree that feeds the last mode (whose MTTKRP gives the fit's
+ * inner product) still reads FP32 rows. */
 int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
+/* G = A^T A in FP64 (R x R, row-major, device) of the device row matrix A
+ * (rows x ldr floats, 16-byte aligned, first R <= 128 columns used, ldr a
+ * multiple of 4): the Gram step of the CP-ALS update, with its per-block
+ * partial sums in workspace the call allocates and frees. Synchronous. */
+int adatm_gram(const float *A, uint64_t rows, int R, int ldr, double *G);
+
 /* Number of kernel launches of one sweep and of one MTTKRP of `mode`. */
 int adatm_engine_launch_counts(adatm_engine *e, uint64_t mode, int *per_sweep, int *per_mttkrp);
 

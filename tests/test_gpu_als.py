@@ -79,3 +79,31 @@ def test_planted_low_rank(gpu):
     e.init_factors(1)
     res = e.als(200, 0.0, graph=True)
     assert res["fit"] > 0.99
+
+
+@pytest.mark.parametrize("rows,R", [(1, 1), (1000, 16), (5000, 32), (20000, 64), (777, 100)])
+def test_gram_device_entry_point(gpu, rows, R):
+    import torch
+    A = gpu
+    ldr = (R + 3) // 4 * 4
+    x = torch.rand(rows, ldr, device="cuda", dtype=torch.float32, generator=torch.Generator("cuda").manual_seed(rows))
+    x[:, R:] = 0
+    G = torch.zeros(R, R, device="cuda", dtype=torch.float64)
+    A.gram_device(x.data_ptr(), rows, R, ldr, G.data_ptr())
+    ref = x[:, :R].double().T @ x[:, :R].double()
+    assert torch.allclose(G, ref, rtol=1e-10, atol=1e-9)
+
+
+def test_bf16_sweep_fit_tracks_fp32(gpu):
+    """BF16 gathers with the fit's MTTKRP in FP32: fit stays finite and close
+    to the FP32 sweep on a skewed 4-mode tensor."""
+    A = gpu
+    t = A.Tensor.generate([5000, 5000, 2000, 500], 3_000_000, alpha=1.1, seed=0)
+    plan, _, _ = A.plan_analytic(t, 32)
+    res = {}
+    for bf in (False, True):
+        e = A.Engine(t, 32, plan, bf16=bf)
+        e.init_factors(0)
+        res[bf] = e.als(8, 0.0, graph=True)["trace"]
+    assert np.all(np.isfinite(res[True]))
+    assert np.max(np.abs(res[True] - res[False])) < 1e-2
