@@ -85,48 +85,45 @@ __global__ void k_frob_final(const double *part, int n, double *out) {
 }
 
 // ---------------------------------------------------------------------------
-// Gram Hadamard + Cholesky + inverse, one block.
+// Gram Hadamard + inverse, one block. V = Hadamard of every G[m], m != mode,
+// is symmetric positive definite, so Gauss-Jordan elimination in place needs
+// no pivoting (each pivot is a diagonal entry of a Schur complement of V,
+// hence positive). All R steps stay in shared memory.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int mode, int R,
                                                       double *X, float *X32) {
-  extern __shared__ double L[];  // R x R
+  extern __shared__ double V[];  // R x R, then the pivot column (R)
+  double *col = V + R * R;
   const int tid = threadIdx.x;
   for (int e = tid; e < R * R; e += blockDim.x) {
     double v = 1.0;
     for (int m = 0; m < nmodes; ++m)
       if (m != mode) v *= g.G[m][e];
-    L[e] = v;
+    V[e] = v;
   }
   __syncthreads();
-  // right-looking Cholesky, lower triangle in place
   for (int j = 0; j < R; ++j) {
-    if (tid == 0) L[j * R + j] = sqrt(L[j * R + j]);
+    const double p = V[j * R + j];
+    for (int i = tid; i < R; i += blockDim.x) col[i] = V[i * R + j];
     __syncthreads();
-    const double djj = L[j * R + j];
-    for (int i = j + 1 + tid; i < R; i += blockDim.x) L[i * R + j] /= djj;
+    // pivot row: V[j][k] = (k == j ? 1 : V[j][k]) / p
+    for (int k = tid; k < R; k += blockDim.x) V[j * R + k] = (k == j ? 1.0 : V[j * R + k]) / p;
     __syncthreads();
-    const int rest = R - j - 1;
-    for (int e = tid; e < rest * rest; e += blockDim.x) {
-      const int i = j + 1 + e / rest, k = j + 1 + e % rest;
-      if (k <= i) L[i * R + k] -= L[i * R + j] * L[k * R + j];
+    // other rows: V[i][k] = (k == j ? 0 : V[i][k]) - col[i] * V[j][k]
+    for (int e = tid; e < R * R; e += blockDim.x) {
+      const int i = e / R, k = e % R;
+      if (i == j) continue;
+      V[e] = (k == j ? 0.0 : V[e]) - col[i] * V[j * R + k];
     }
     __syncthreads();
   }
-  // column c of the inverse: forward solve L y = e_c, backward L^T x = y
-  for (int c = tid; c < R; c += blockDim.x) {
-    for (int i = 0; i < R; ++i) {
-      double t = (i == c) ? 1.0 : 0.0;
-      for (int k = 0; k < i; ++k) t -= L[i * R + k] * X[k * R + c];
-      X[i * R + c] = t / L[i * R + i];
-    }
-    for (int i = R - 1; i >= 0; --i) {
-      double t = X[i * R + c];
-      for (int k = i + 1; k < R; ++k) t -= L[k * R + i] * X[k * R + c];
-      X[i * R + c] = t / L[i * R + i];
-    }
+  for (int e = tid; e < R * R; e += blockDim.x) {
+    // symmetrise: the two triangles differ only by rounding
+    const int i = e / R, k = e % R;
+    const double v = 0.5 * (V[e] + V[k * R + i]);
+    X[e] = v;
+    X32[e] = (float)v;
   }
-  __syncthreads();
-  for (int e = tid; e < R * R; e += blockDim.x) X32[e] = (float)X[e];
 }
 
 // ---------------------------------------------------------------------------
@@ -224,35 +221,58 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
 
 // Sum the partial Grams; with lam != nullptr also derive lambda (2-norm on the
 // first iteration, max-norm floored at 1 after) and scale G by 1/(l_r l_s).
-__global__ void k_finalize(const double *part_gram, const double *part_max, int nblocks, int R,
-                           double *G, double *lam, const int *iter) {
+// Grid: ceil(R*R / kFinEntries) blocks of 256 threads; a block sums
+// kFinEntries entries, its 256 / kFinEntries warps splitting the partials, so
+// no thread walks a long chain of dependent L2 loads. Every block derives the
+// lambda values it needs; block 0 stores them.
+constexpr int kFinEntries = 32;
+constexpr int kFinParts = 256 / kFinEntries;
+
+__global__ void __launch_bounds__(256) k_finalize(const double *part_gram, const double *part_max,
+                                                  int nblocks, int R, double *G, double *lam,
+                                                  const int *iter) {
   __shared__ double slam[128];
+  __shared__ double red[256];
   const int tid = threadIdx.x;
-  const bool first = (iter == nullptr) || (*iter == 0);
-  for (int r = tid; r < R; r += blockDim.x) {
-    if (lam) {
-      double v;
+  if (lam) {
+    const bool first = (iter == nullptr) || (*iter == 0);
+    const int parts = 256 / R;  // R <= 128
+    const int r = tid % R, q = tid / R;
+    double v = 0.0;
+    if (q < parts) {
       if (first) {
-        double s = 0;
-        for (int b = 0; b < nblocks; ++b) s += part_gram[(size_t)b * R * R + r * R + r];
-        v = sqrt(s);
+        for (int b = q; b < nblocks; b += parts) v += part_gram[(size_t)b * R * R + r * R + r];
       } else {
-        double mx = 0;
-        for (int b = 0; b < nblocks; ++b) mx = fmax(mx, part_max[(size_t)b * R + r]);
-        v = fmax(mx, 1.0);
+        for (int b = q; b < nblocks; b += parts) v = fmax(v, part_max[(size_t)b * R + r]);
       }
-      slam[r] = v;
-      lam[r] = v;
     }
+    red[tid] = v;
+    __syncthreads();
+    if (tid < R) {
+      double a = 0.0;
+      for (int k = 0; k < parts; ++k) a = first ? a + red[k * R + tid] : fmax(a, red[k * R + tid]);
+      const double l = first ? sqrt(a) : fmax(a, 1.0);
+      slam[tid] = l;
+      if (blockIdx.x == 0) lam[tid] = l;
+    }
+    __syncthreads();
   }
+  const int e = blockIdx.x * kFinEntries + tid % kFinEntries;
+  const int q = tid / kFinEntries;
+  double acc = 0.0;
+  if (e < R * R)
+    for (int b = q; b < nblocks; b += kFinParts) acc += part_gram[(size_t)b * R * R + e];
+  red[tid] = acc;
   __syncthreads();
-  for (int e = tid; e < R * R; e += blockDim.x) {
-    double s = 0;
-    for (int b = 0; b < nblocks; ++b) s += part_gram[(size_t)b * R * R + e];
-    if (lam) s /= slam[e / R] * slam[e % R];
-    G[e] = s;
+  if (tid < kFinEntries && e < R * R) {
+    double sum = 0.0;
+    for (int k = 0; k < kFinParts; ++k) sum += red[k * kFinEntries + tid];
+    if (lam) sum /= slam[e / R] * slam[e % R];
+    G[e] = sum;
   }
 }
+
+int finalize_blocks(int R) { return (R * R + kFinEntries - 1) / kFinEntries; }
 
 // A /= lambda (fp32), bf16 copy, optional partial <A, M> per column.
 template <int LANES>
@@ -322,11 +342,14 @@ __global__ void k_fit(GramSet g, int nmodes, int R, const double *lam, const dou
     for (int m = 0; m < nmodes; ++m) h *= g.G[m][e];
     nrm += h * lam[e / R] * lam[e % R];
   }
+  // <X, Z> = sum_r lam_r sum_b part_inner[b][r]: 256 / R threads per column
   double inner = 0;
-  for (int r = tid; r < R; r += blockDim.x) {
-    double s = 0;
-    for (int b = 0; b < nblocks; ++b) s += part_inner[(size_t)b * R + r];
-    inner += s * lam[r];
+  {
+    const int parts = 256 / R, r = tid % R, q = tid / R;
+    if (q < parts) {
+      for (int b = q; b < nblocks; b += parts) inner += part_inner[(size_t)b * R + r];
+      inner *= lam[r];
+    }
   }
   red[tid] = nrm;
   __syncthreads();
@@ -386,7 +409,15 @@ void set_attributes() {
   ADATM_CUDA(cudaFuncSetAttribute(k_update<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)update_smem<32>()));
   ADATM_CUDA(cudaFuncSetAttribute(k_gram_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  128 * 128 * (int)sizeof(double)));
+                                  (128 * 128 + 128) * (int)sizeof(double)));
+}
+
+// Row blocks of the update: enough to give every block at least one full
+// batch of rows, at most the workspace's partial slots.
+int update_blocks(uint64_t rows, int R, int max_blocks) {
+  const uint64_t groups = 256 / lanes_for(R);
+  const uint64_t need = (rows + groups - 1) / groups;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)max_blocks, need));
 }
 
 void run_update(const UpdArgs &u, int nblocks, cudaStream_t s) {
@@ -432,8 +463,9 @@ void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, 
   u.ldr = ldr;
   u.part_gram = w.part_gram.get();
   u.part_max = w.part_max.get();
-  run_update(u, w.nblocks, s);
-  k_finalize<<<1, 256, 0, s>>>(w.part_gram.get(), w.part_max.get(), w.nblocks, R, G, nullptr,
+  const int nb = update_blocks(rows, R, w.nblocks);
+  run_update(u, nb, s);
+  k_finalize<<<finalize_blocks(R), 256, 0, s>>>(w.part_gram.get(), w.part_max.get(), nb, R, G, nullptr,
                                nullptr);
   ADATM_LAUNCH();
 }
@@ -449,7 +481,7 @@ void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s) {
 }
 
 void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s) {
-  const size_t smem = (size_t)w.R * w.R * sizeof(double);
+  const size_t smem = (size_t)(w.R * w.R + w.R) * sizeof(double);
   k_gram_inverse<<<1, 256, smem, s>>>(g, w.nmodes, mode, w.R, w.vinv64.get(), w.vinv32.get());
   ADATM_LAUNCH();
 }
@@ -465,8 +497,9 @@ void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, d
   u.ldr = w.ldr;
   u.part_gram = w.part_gram.get();
   u.part_max = w.part_max.get();
-  run_update(u, w.nblocks, s);
-  k_finalize<<<1, 256, 0, s>>>(w.part_gram.get(), w.part_max.get(), w.nblocks, w.R, G_mode,
+  const int nb = update_blocks(rows, w.R, w.nblocks);
+  run_update(u, nb, s);
+  k_finalize<<<finalize_blocks(w.R), 256, 0, s>>>(w.part_gram.get(), w.part_max.get(), nb, w.R, G_mode,
                                w.lambda.get(), w.iter.get());
   ADATM_LAUNCH();
   double *pi = inner ? w.part_inner.get() : nullptr;
