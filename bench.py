@@ -54,14 +54,15 @@ def peaks():
     return FALLBACK_HBM, "fallback"
 
 
-def profiled_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/mttkrp_walk.md, line 'traffic_bytes_per_launch: X')."""
+def profiled_traffic(mode):
+    """Per-launch DRAM bytes of mode `mode`'s MTTKRP from the committed ncu
+    summary (profiles/mttkrp_walk.md, line 'traffic_bytes_per_launch[mode M]: X')."""
     p = os.path.join(HERE, "profiles", "mttkrp_walk.md")
     if not os.path.exists(p):
         return None
+    key = f"traffic_bytes_per_launch[mode {mode}]:"
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -298,7 +299,7 @@ def run_ours(args):
     peak, peak_kind = peaks()
     seq_bytes = sum(eng.mttkrp_bytes(m) for m in range(nmodes))
     seq_gbs = seq_bytes / (sum(mode_ms) * 1e-3) / 1e9
-    traffic = profiled_traffic()
+    traffic = profiled_traffic(dom)
 
     # plain GPU rCSF (one tree per mode, no memo) and BF16 gathers, same GPU
     plain = A.Engine(t, RANK, A.plan_splatt(t, A.CSF_ALLMODE))
