@@ -149,6 +149,7 @@ _SIGS = [
     ("adatm_engine_fit", C.c_int, [C.c_void_p, P_f64]),
     ("adatm_engine_mttkrp_bytes", C.c_int, [C.c_void_p, u64, P_f64]),
     ("adatm_gram", C.c_int, [C.c_void_p, u64, C.c_int, C.c_int, C.c_void_p]),
+    ("adatm_gram_noalloc", C.c_int, [C.c_void_p, u64, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     ("adatm_engine_launch_counts", C.c_int, [C.c_void_p, u64, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
 ]
 

@@ -1,5 +1,6 @@
 // als.cu -- dense CP-ALS kernels (see als.cuh).
 #include <algorithm>
+#include <mutex>
 
 #include "als.cuh"
 
@@ -515,6 +516,92 @@ void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, d
 void fit(const GramSet &g, AlsWork &w, cudaStream_t s) {
   k_fit<<<1, 256, 0, s>>>(g, w.nmodes, w.R, w.lambda.get(), w.part_inner.get(), w.nblocks,
                           w.scalars.get(), w.fit_trace.get(), w.max_trace, w.iter.get());
+  ADATM_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// G = A^T A without any device allocation.
+//
+// For callers that cannot allocate device memory at the point of the call:
+// a host whose caching allocator already holds nearly all of HBM (cudaMalloc
+// would fail there), or a loop that must not pay cudaFree's implicit
+// device-wide synchronisation. The per-block partial Grams and column maxima
+// live in a fixed file-scope device array instead of an AlsWork, which bounds
+// the rank to kNoallocMaxR columns and the row blocks to kNoallocBlocks.
+//
+// Every block of k_update writes its whole partial before k_finalize reads
+// it, so nothing in the scratch has to start at zero. The scratch is shared
+// by all calls on one device: calls that overlap in time (two host threads,
+// or streams not ordered against each other) race on it. The first call on a
+// device resolves the scratch address (and sets kernel attributes), which is
+// set-up work a caller should do once before any stream capture.
+// ---------------------------------------------------------------------------
+constexpr int kNoallocMaxR = 64;
+constexpr int kNoallocBlocks = 64;
+constexpr size_t kNoallocGramDoubles = (size_t)kNoallocBlocks * kNoallocMaxR * kNoallocMaxR;
+constexpr size_t kNoallocDoubles = kNoallocGramDoubles + (size_t)kNoallocBlocks * kNoallocMaxR;
+constexpr int kNoallocMaxDevices = 64;
+
+// 2 MiB of partial Grams + 32 KiB of column maxima.
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocDoubles];
+
+namespace {
+
+struct NoallocSlot {
+  std::once_flag once;
+  double *ptr = nullptr;
+  cudaError_t err = cudaSuccess;
+};
+NoallocSlot g_noalloc_slots[kNoallocMaxDevices];
+
+// Device address of the scratch on the current device (resolved once).
+double *noalloc_scratch() {
+  int dev = 0;
+  ADATM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoallocMaxDevices) throw BadInput("device ordinal above the scratch table");
+  NoallocSlot &slot = g_noalloc_slots[dev];
+  std::call_once(slot.once, [&] {
+    void *p = nullptr;
+    slot.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (slot.err == cudaSuccess) {
+      try {
+        set_attributes();
+      } catch (const CudaError &) {
+        slot.err = cudaGetLastError();
+        if (slot.err == cudaSuccess) slot.err = cudaErrorUnknown;
+      }
+    }
+    slot.ptr = static_cast<double *>(p);
+  });
+  if (slot.err != cudaSuccess)
+    throw CudaError(std::string("scratch set-up failed: ") + cudaGetErrorString(slot.err));
+  return slot.ptr;
+}
+
+}  // namespace
+
+int gram_noalloc_max_rank() { return kNoallocMaxR; }
+
+void gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, cudaStream_t s) {
+  if (R < 1 || R > kNoallocMaxR)
+    throw BadInput("adatm_gram_noalloc: R = " + std::to_string(R) + " is outside 1.." +
+                   std::to_string(kNoallocMaxR) + ", the columns its fixed scratch holds");
+  if (ldr < R || ldr % 4 != 0) throw BadInput("adatm_gram_noalloc: ldr must be >= R and a multiple of 4");
+  if (((uintptr_t)A & 15) != 0) throw BadInput("adatm_gram_noalloc: A must be 16-byte aligned");
+  double *scratch = noalloc_scratch();
+  UpdArgs u;
+  u.M = A;
+  u.vinv = nullptr;
+  u.A = nullptr;
+  u.rows = rows;
+  u.R = R;
+  u.ldr = ldr;
+  u.part_gram = scratch;
+  u.part_max = scratch + kNoallocGramDoubles;
+  const int nb = update_blocks(rows, R, kNoallocBlocks);
+  run_update(u, nb, s);
+  k_finalize<<<finalize_blocks(R), 256, 0, s>>>(u.part_gram, u.part_max, nb, R, G, nullptr,
+                                                nullptr);
   ADATM_LAUNCH();
 }
 

@@ -47,6 +47,11 @@ void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, d
 // fit = 1 - sqrt(||X||^2 + ||Z||^2 - 2<X,Z>) / ||X||, stored in
 // w.scalars[1] and w.fit_trace[iter]; advances w.iter.
 void fit(const GramSet &g, AlsWork &w, cudaStream_t s);
+// G = A^T A in FP64 like gram(), with its partial sums in a fixed device
+// array instead of an AlsWork: no device allocation. R <= gram_noalloc_max_rank();
+// calls that overlap in time on one device race on the shared array.
+void gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, cudaStream_t s);
+int gram_noalloc_max_rank();
 // Convert fp32 rows to bf16 (rows x ldr).
 void to_bf16(const float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s);
 

@@ -1156,6 +1156,14 @@ int adatm_gram(const float *A, uint64_t rows, int R, int ldr, double *G) {
   });
 }
 
+int adatm_gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, void *stream) {
+  return guarded([&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    gram_noalloc(A, rows, R, ldr, G, s);
+    ADATM_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 int adatm_engine_launch_counts(adatm_engine *e, uint64_t mode, int *per_sweep, int *per_mttkrp) {
   return guarded([&] {
     if (per_sweep) *per_sweep = e->eng->kernels_per_sweep();

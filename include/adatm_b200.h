@@ -259,6 +259,17 @@ int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
  * partial sums in workspace the call allocates and frees. Synchronous. */
 int adatm_gram(const float *A, uint64_t rows, int R, int ldr, double *G);
 
+/* adatm_gram without any device allocation; no counterpart in the reference.
+ * For callers that cannot allocate device memory at the call (a caching
+ * allocator already holds the free HBM, or cudaFree's device-wide
+ * synchronisation is not acceptable): the partial sums live in a fixed
+ * 2 MiB device array, so R must be <= 64 (SPLATT_ERROR_BADINPUT otherwise).
+ * Runs on `stream` (a cudaStream_t; NULL = the legacy default stream) and
+ * returns after it completes. Calls that overlap in time on one device race
+ * on the shared array. The first call on a device resolves the array's
+ * address; make it once before any stream capture. */
+int adatm_gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, void *stream);
+
 /* Number of kernel launches of one sweep and of one MTTKRP of `mode`. */
 int adatm_engine_launch_counts(adatm_engine *e, uint64_t mode, int *per_sweep, int *per_mttkrp);
 
