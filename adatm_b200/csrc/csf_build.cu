@@ -24,7 +24,7 @@ namespace adatm {
 
 size_t DevCsf::device_bytes() const {
   size_t b = vals64.bytes() + vals32.bytes();
-  for (int l = 0; l < kMaxModes; ++l) b += fptr[l].bytes() + fids[l].bytes();
+  for (int l = 0; l < kMaxModes; ++l) b += fptr[l].bytes() + fids[l].bytes() + cdepth[l].bytes();
   return b;
 }
 
@@ -473,6 +473,31 @@ void count_levels(const SortBufs<W> &b, uint64_t n, const KeySpec &spec, DevBuf<
   nfibs[nl] = n;
 }
 
+// Close depths of level l's nodes from level l-1's: the last child of every
+// parent p gets 1 + (close depth of p). Launched for l = 1..N-1 in order.
+__global__ void k_close_depth(const uint32_t *fptr_parent, uint64_t nparent,
+                              const uint8_t *cd_parent, uint8_t *cd_child) {
+  const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nparent) return;
+  const uint32_t last = fptr_parent[p + 1] - 1;
+  cd_child[last] = (uint8_t)(1 + (cd_parent ? cd_parent[p] : 0));
+}
+
+void build_close_depths(DevCsf &out, cudaStream_t s) {
+  const int N = out.nmodes;
+  for (int l = 1; l < N; ++l) {
+    const uint64_t n = l == N - 1 ? out.nnz : out.nfibs[l];
+    out.cdepth[l].alloc(n);
+    if (n == 0) continue;
+    ADATM_CUDA(cudaMemsetAsync(out.cdepth[l].get(), 0, n, s));
+    const uint64_t np = out.nfibs[l - 1];
+    k_close_depth<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(
+        out.fptr[l - 1].get(), np, l >= 2 ? out.cdepth[l - 1].get() : nullptr,
+        out.cdepth[l].get());
+    ADATM_LAUNCH();
+  }
+}
+
 template <int W>
 void build_w(const DevCoo &coo, const uint64_t *perm, const KeySpec &spec, DevCsf &out,
              cudaStream_t s) {
@@ -508,6 +533,7 @@ void build_w(const DevCoo &coo, const uint64_t *perm, const KeySpec &spec, DevCs
   ADATM_CUDA(cudaMemcpyAsync(totals.get(), ht, sizeof(ht), cudaMemcpyHostToDevice, s));
   k_level_tails<<<1, 32, 0, s>>>(lo, totals.get(), N - 1, n);
   ADATM_LAUNCH();
+  build_close_depths(out, s);
   ADATM_CUDA(cudaStreamSynchronize(s));
 }
 

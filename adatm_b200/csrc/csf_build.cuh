@@ -27,6 +27,12 @@ struct DevCsf {
   DevBuf<uint32_t> fids[kMaxModes];    // levels 0..N-1 (0 = root ids)
   DevBuf<double> vals64;               // leaf values, FP64 (bit-exact copy)
   DevBuf<float> vals32;                // leaf values, FP32 (compute copy)
+  // Close depth of every node of levels 1..N-1: how many ancestor levels end
+  // together with it (0 = not the last child of its parent; 1 = last child,
+  // its parent not the last child of its own parent; ...). A walk that reads
+  // it knows where every node of every level above closes without touching
+  // fptr.
+  DevBuf<uint8_t> cdepth[kMaxModes];
   size_t device_bytes() const;
 };
 

@@ -13,8 +13,8 @@ namespace adatm {
 
 struct EngineOptions {
   FactorType factor_type = FactorType::F32;
-  uint32_t chunk_leaf = 32;   // source units per chunk, nonzero sources
-  uint32_t chunk_rows = 16;   // source units per chunk, memo-row sources
+  uint32_t chunk_leaf = 256;  // source units per chunk (one warp), nonzero sources
+  uint32_t chunk_rows = 128;  // source units per chunk (one warp), memo-row sources
   int max_iters = 1024;       // capacity of the device fit trace
 };
 

@@ -1,5 +1,6 @@
 // mttkrp.cu -- tree-walk MTTKRP kernels (see mttkrp.cuh for the scheme).
 #include <algorithm>
+#include <type_traits>
 
 #include "mttkrp.cuh"
 
@@ -15,381 +16,596 @@ struct WalkArgs {
   const uint32_t *fptr[kMaxModes];
   const uint32_t *fids[kMaxModes];
   const float *vals;
-  const float *src_rows;
-  const uint32_t *src_ids;     // fids of the source level (S)
+  const float *src_rows;       // memo rows of the source level (S < N-1)
+  const uint32_t *src_ids;     // fids of the source level
+  const uint8_t *src_cd;       // close depths of the source level (S >= 1)
   const void *U_src;           // factor rows of the source level
-  const uint32_t *out_ids;     // fids of the output level (d)
-  const uint32_t *par_fptr;    // fptr of level S-1
-  const uint32_t *par_fids;    // fids of level S-1
-  const void *U_par;           // factor rows of level S-1
-  float *par_store;            // memo rows of level S-1 (or null)
-  uint64_t par_n;              // nodes of level S-1
   const void *U[kMaxModes];
   float *store[kMaxModes];
   float *out;
   const uint32_t *sched;
 };
 
-__device__ __forceinline__ float4 f4_zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
-__device__ __forceinline__ float4 f4_mul(float4 a, float4 b) {
-  return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w);
+// ---------------------------------------------------------------------------
+// Warp-uniform tree walk.
+//
+// One warp walks one chunk of consecutive source units; its 32 lanes split
+// the R columns (V = 1, 2 or 4 columns per lane), so every lane follows the
+// same control flow and each factor-row gather is one coalesced access. Units
+// go in batches of 32 (one per lane for the index loads): the batch's factor
+// rows are gathered with many loads in flight, then summed in order into the
+// open node of level S-1. Where a node closes is read from the tree's close
+// depths (no fptr traffic): a unit with close depth c closes its ancestors at
+// levels S-1 .. S-c. The nodes of level S-1 that close in the batch become
+// the items of the next level up -- their sums sit in shared memory, are
+// multiplied by their own factor rows and summed into level S-2 nodes in the
+// same way -- until level d, where completed nodes go to the output.
+// ---------------------------------------------------------------------------
+constexpr int kWarps = 8;   // warps (chunks) per block
+constexpr int kBatch = 32;  // source units per batch
+
+template <int V>
+struct alignas(sizeof(float) * V) fv {
+  float x[V];
+};
+
+template <int V>
+__device__ __forceinline__ fv<V> fv_fill(float s) {
+  fv<V> r;
+#pragma unroll
+  for (int i = 0; i < V; ++i) r.x[i] = s;
+  return r;
 }
-__device__ __forceinline__ float4 f4_scale(float s, float4 a) {
-  return make_float4(s * a.x, s * a.y, s * a.z, s * a.w);
+template <int V>
+__device__ __forceinline__ void fv_axpy(fv<V> &acc, float s, const fv<V> &b) {
+#pragma unroll
+  for (int i = 0; i < V; ++i) acc.x[i] = fmaf(s, b.x[i], acc.x[i]);
 }
-__device__ __forceinline__ void f4_fma(float4 &acc, float4 a, float4 b) {
-  acc.x = fmaf(a.x, b.x, acc.x);
-  acc.y = fmaf(a.y, b.y, acc.y);
-  acc.z = fmaf(a.z, b.z, acc.z);
-  acc.w = fmaf(a.w, b.w, acc.w);
+template <int V>
+__device__ __forceinline__ void fv_fma(fv<V> &acc, const fv<V> &a, const fv<V> &b) {
+#pragma unroll
+  for (int i = 0; i < V; ++i) acc.x[i] = fmaf(a.x[i], b.x[i], acc.x[i]);
 }
-__device__ __forceinline__ void f4_add(float4 &acc, float4 a) {
-  acc.x += a.x;
-  acc.y += a.y;
-  acc.z += a.z;
-  acc.w += a.w;
+template <int V>
+__device__ __forceinline__ fv<V> fv_mul(const fv<V> &a, const fv<V> &b) {
+  fv<V> r;
+#pragma unroll
+  for (int i = 0; i < V; ++i) r.x[i] = a.x[i] * b.x[i];
+  return r;
+}
+template <int V>
+__device__ __forceinline__ fv<V> fv_scale(float s, const fv<V> &a) {
+  fv<V> r;
+#pragma unroll
+  for (int i = 0; i < V; ++i) r.x[i] = s * a.x[i];
+  return r;
 }
 
-template <FactorType FT>
-__device__ __forceinline__ float4 load_row(const void *U, uint32_t row, int ldr, int col, bool act) {
-  if (!act) return f4_zero();
+// Columns col..col+V-1 of factor row `row` (FP32 or BF16 storage).
+template <int V, FactorType FT>
+__device__ __forceinline__ fv<V> ld_factor(const void *U, uint32_t row, int ldr, int col, bool act) {
+  fv<V> r = fv_fill<V>(0.f);
+  if (!act) return r;
   if constexpr (FT == FactorType::F32) {
-    return __ldg(reinterpret_cast<const float4 *>(static_cast<const float *>(U) + (size_t)row * ldr + col));
+    const float *p = static_cast<const float *>(U) + (size_t)row * ldr + col;
+    if constexpr (V == 1) {
+      r.x[0] = __ldg(p);
+    } else if constexpr (V == 2) {
+      const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+      r.x[0] = t.x;
+      r.x[1] = t.y;
+    } else {
+      const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+      r.x[0] = t.x;
+      r.x[1] = t.y;
+      r.x[2] = t.z;
+      r.x[3] = t.w;
+    }
   } else {
-    const uint2 raw = __ldg(reinterpret_cast<const uint2 *>(
-        static_cast<const __nv_bfloat16 *>(U) + (size_t)row * ldr + col));
-    const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&raw.x));
-    const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&raw.y));
-    return make_float4(lo.x, lo.y, hi.x, hi.y);
+    const __nv_bfloat16 *p = static_cast<const __nv_bfloat16 *>(U) + (size_t)row * ldr + col;
+    if constexpr (V == 1) {
+      r.x[0] = __bfloat162float(__ldg(p));
+    } else if constexpr (V == 2) {
+      const float2 t = __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162 *>(p)));
+      r.x[0] = t.x;
+      r.x[1] = t.y;
+    } else {
+      const uint2 raw = __ldg(reinterpret_cast<const uint2 *>(p));
+      const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&raw.x));
+      const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&raw.y));
+      r.x[0] = lo.x;
+      r.x[1] = lo.y;
+      r.x[2] = hi.x;
+      r.x[3] = hi.y;
+    }
   }
+  return r;
 }
 
-__device__ __forceinline__ float4 load_f4(const float *p, uint64_t row, int ldr, int col, bool act) {
-  if (!act) return f4_zero();
-  return __ldg(reinterpret_cast<const float4 *>(p + row * (uint64_t)ldr + col));
-}
-
-__device__ __forceinline__ void store_f4(float *p, uint64_t row, int ldr, int col, float4 v, bool act) {
-  if (act) *reinterpret_cast<float4 *>(p + row * (uint64_t)ldr + col) = v;
-}
-
-__device__ __forceinline__ void atomic_f4(float *p, uint64_t row, int ldr, int col, float4 v, bool act) {
-  if (act) atomicAdd(reinterpret_cast<float4 *>(p + row * (uint64_t)ldr + col), v);
-}
-
-// Units of the source level walked per batch. A batch first stages what it
-// needs -- the ids (and values) of its B units, and a window with the ids and
-// child ends of the B parent nodes (level S-1) it can touch -- in per-group
-// shared memory, then issues all factor-row loads at once (the B unit
-// products and the B window rows), and only then walks the units. The walk
-// keeps the parent level in registers; the levels above it live in a
-// local-memory struct that only the rarer completions of level S-2 touch,
-// through out-of-line functions, so the loop body stays small enough for the
-// instruction cache. All cross-lane traffic goes through shared memory
-// between __syncwarp fences.
-constexpr int kBatch = 8;
-
-struct GroupMeta {
-  uint32_t id[kBatch];
-  float v[kBatch];
-  uint32_t wfid[kBatch];
-  uint32_t wend[kBatch];
-  uint32_t pad;  // 132-byte stride: the groups of a warp start on different banks
-};
-
-template <int LANES>
-constexpr size_t walk_smem() {
-  return (size_t)(256 / LANES) * (2 * kBatch * LANES * sizeof(float4) + sizeof(GroupMeta));
-}
-
-// State of the levels above the source's parent level.
-struct Upper {
-  uint32_t node[kMaxModes];
-  uint32_t endc[kMaxModes];
-  uint32_t part;     // bit l: the level-l node began before the chunk
-  uint32_t touched;  // bit l: acc[l] holds contributions
-  float4 acc[kMaxModes];
-  float4 P[kMaxModes];  // P_l = U_0[root] * ... * U_l[fids[l][node[l]]]
-};
-
-// P_l for levels from..lim-1.
-template <FactorType FT>
-__device__ __noinline__ void upper_prefix(const WalkArgs &a, Upper &u, int from, int lim, int col,
-                                          bool act) {
-  for (int l = from; l < lim; ++l) {
-    const float4 row = load_row<FT>(a.U[l], a.fids[l][u.node[l]], a.ldr, col, act);
-    u.P[l] = l == 0 ? row : f4_mul(u.P[l - 1], row);
+// FP32 row matrices (memo rows, outputs).
+template <int V>
+__device__ __forceinline__ fv<V> ld_rows(const float *base, uint64_t row, int ldr, int col, bool act) {
+  fv<V> r = fv_fill<V>(0.f);
+  if (!act) return r;
+  const float *p = base + row * (uint64_t)ldr + col;
+  if constexpr (V == 1) {
+    r.x[0] = __ldg(p);
+  } else if constexpr (V == 2) {
+    const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+    r.x[0] = t.x;
+    r.x[1] = t.y;
+  } else {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    r.x[0] = t.x;
+    r.x[1] = t.y;
+    r.x[2] = t.z;
+    r.x[3] = t.w;
   }
+  return r;
 }
 
-template <FactorType FT>
-__device__ __noinline__ void upper_init(const WalkArgs &a, Upper &u, const uint32_t *sc, int col,
+template <int V>
+__device__ __forceinline__ void st_rows(float *base, uint64_t row, int ldr, int col, const fv<V> &v,
                                         bool act) {
-  u.part = sc[a.S];
-  u.touched = 0;
-  for (int l = 0; l < a.S; ++l) {
-    u.node[l] = sc[l];
-    u.endc[l] = a.fptr[l][u.node[l] + 1];
-    u.acc[l] = f4_zero();
+  if (!act) return;
+  float *p = base + row * (uint64_t)ldr + col;
+  if constexpr (V == 1) {
+    *p = v.x[0];
+  } else if constexpr (V == 2) {
+    *reinterpret_cast<float2 *>(p) = make_float2(v.x[0], v.x[1]);
+  } else {
+    *reinterpret_cast<float4 *>(p) = make_float4(v.x[0], v.x[1], v.x[2], v.x[3]);
   }
-  upper_prefix<FT>(a, u, 0, min(a.d, a.S - 1), col, act);
 }
 
-// The node of level p = S-2 completed; its sum is accP (or u.acc). Emit it and
-// every ancestor that completes with it; advance the path; refresh P.
-template <FactorType FT>
-__device__ __noinline__ void upper_complete(const WalkArgs &a, Upper &u, float4 accP, int col,
-                                            bool act) {
-  const int d = a.d;
-  int pchange = kMaxModes;
-  bool carry = true;
-  for (int l = a.S - 2; l >= 0 && carry; --l) {
-    if (l >= d) {
-      const float4 v = (l == a.S - 2) ? accP : u.acc[l];
-      const bool part = (u.part >> l) & 1u;
-      if (a.store[l] != nullptr) {
-        if (part) atomic_f4(a.store[l], u.node[l], a.ldr, col, v, act);
-        else store_f4(a.store[l], u.node[l], a.ldr, col, v, act);
+template <int V>
+__device__ __forceinline__ void red_rows(float *base, uint64_t row, int ldr, int col, const fv<V> &v,
+                                         bool act) {
+  if (!act) return;
+  float *p = base + row * (uint64_t)ldr + col;
+  if constexpr (V == 1) {
+    atomicAdd(p, v.x[0]);
+  } else if constexpr (V == 2) {
+    atomicAdd(reinterpret_cast<float2 *>(p), make_float2(v.x[0], v.x[1]));
+  } else {
+    atomicAdd(reinterpret_cast<float4 *>(p), make_float4(v.x[0], v.x[1], v.x[2], v.x[3]));
+  }
+}
+
+// Factor-row gathers through a per-lane base pointer (the lane's first
+// column) and a byte stride, so an address is one wide multiply-add.
+template <int V, FactorType FT>
+struct RowSrc {
+  const char *base = nullptr;
+  uint32_t stride = 0;
+  __device__ __forceinline__ RowSrc(const void *U, int ldr, int col) {
+    constexpr int esz = FT == FactorType::F32 ? 4 : 2;
+    base = static_cast<const char *>(U) + (size_t)col * esz;
+    stride = (uint32_t)ldr * esz;
+  }
+  __device__ __forceinline__ fv<V> load(uint32_t row, bool on) const {
+    fv<V> r = fv_fill<V>(0.f);
+    if (!on) return r;
+    const char *p = base + (size_t)row * stride;
+    if constexpr (FT == FactorType::F32) {
+      if constexpr (V == 1) {
+        r.x[0] = __ldg(reinterpret_cast<const float *>(p));
+      } else if constexpr (V == 2) {
+        const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+        r.x[0] = t.x;
+        r.x[1] = t.y;
+      } else {
+        const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+        r.x[0] = t.x;
+        r.x[1] = t.y;
+        r.x[2] = t.z;
+        r.x[3] = t.w;
+      }
+    } else {
+      if constexpr (V == 1) {
+        r.x[0] = __bfloat162float(__ldg(reinterpret_cast<const __nv_bfloat16 *>(p)));
+      } else if constexpr (V == 2) {
+        const float2 t = __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162 *>(p)));
+        r.x[0] = t.x;
+        r.x[1] = t.y;
+      } else {
+        const uint2 raw = __ldg(reinterpret_cast<const uint2 *>(p));
+        const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&raw.x));
+        const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&raw.y));
+        r.x[0] = lo.x;
+        r.x[1] = lo.y;
+        r.x[2] = hi.x;
+        r.x[3] = hi.y;
+      }
+    }
+    return r;
+  }
+};
+
+// Shared memory of one contraction warp: kBatch item rows, a carry row per
+// level (the open node's partial sum) and a prefix row per level (P_l = U_0
+// [node_0] * ... * U_l[node_l] for the levels above d), all in fv<V> slots of
+// 32 lanes; then the batch's (id, value) pairs, the factor-row ids of the
+// parent nodes that close in the batch, and a 32-word exchange buffer.
+constexpr int kSlots = kBatch + 2 * kMaxModes;
+
+template <int V>
+constexpr size_t contract_warp_smem() {
+  return (size_t)kSlots * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint2) + 2 * sizeof(uint32_t));
+}
+template <int V>
+constexpr size_t contract_smem() {
+  return (size_t)kWarps * contract_warp_smem<V>();
+}
+
+// Recompute the prefix rows of levels lo..hi-1 from the node indices (lane l
+// of nodeL holds the node of level l).
+template <int V, FactorType FT>
+__device__ __noinline__ void refresh_prefix(const WalkArgs &a, fv<V> *pre, uint32_t nodeL, int lo,
+                                            int hi, int col, bool act, int lane) {
+  for (int l = lo; l < hi; ++l) {
+    const uint32_t n = __shfl_sync(~0u, nodeL, l);
+    const bool valid = (uint64_t)n < a.nfibs[l];
+    const uint32_t f = valid ? __ldg(a.fids[l] + n) : 0u;
+    const fv<V> row = ld_factor<V, FT>(a.U[l], f, a.ldr, col, act && valid);
+    pre[l * 32 + lane] = l == 0 ? row : fv_mul(pre[(l - 1) * 32 + lane], row);
+  }
+}
+
+// Levels lo..hi-1 move on to their next node (their nodes closed); their
+// prefix rows are recomputed. Returns the updated per-lane node register.
+template <int V, FactorType FT>
+__device__ __noinline__ uint32_t advance_prefix(const WalkArgs &a, fv<V> *pre, uint32_t nodeL,
+                                                int lo, int hi, int col, bool act, int lane) {
+  if (lane >= lo && lane < hi) nodeL += 1;
+  if (lo < hi && (uint64_t)__shfl_sync(~0u, nodeL, lo) < a.nfibs[lo])
+    refresh_prefix<V, FT>(a, pre, nodeL, lo, hi, col, act, lane);
+  return nodeL;
+}
+
+// Compaction of per-lane values onto the set bits of m: lane i gets the
+// value of the lane holding the i-th set bit (i < popc(m)), else 0.
+__device__ __forceinline__ uint32_t compact_bits(uint32_t m, uint32_t value, uint32_t *xbuf, int lane) {
+  if ((m >> lane) & 1u) xbuf[__popc(m & lanemask_lt())] = value;
+  __syncwarp();
+  const uint32_t r = lane < __popc(m) ? xbuf[lane] : 0u;
+  __syncwarp();
+  return r;
+}
+
+// Contraction (S > d).
+//
+// The source units of a batch are summed into the open node of level S-1
+// (carry `acc`, in registers). With FUSE (S-1 > d and no memo store at level
+// S-1), a unit that closes its level-(S-1) node also multiplies the node's sum
+// by the node's own factor row -- gathered, for the closing units only, in
+// the same batch of loads -- and adds it to the open node of level S-2 (carry
+// `acc2`, in registers); the nodes of level S-2 that close become the items
+// of the level loop. Without FUSE the closed level-(S-1) nodes are the items.
+// The level loop takes the items up one level at a time (memo stores, factor
+// rows, carries of the levels above in shared memory) until level d.
+template <int V, FactorType FT, bool LEAF, bool FUSE>
+__global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ WalkArgs a) {
+  extern __shared__ __align__(16) unsigned char walk_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t chunk_id = blockIdx.x * kWarps + warp;
+  if (chunk_id >= a.nchunks) return;
+  unsigned char *wbase = walk_raw + (size_t)warp * contract_warp_smem<V>();
+  fv<V> *items = reinterpret_cast<fv<V> *>(wbase);
+  fv<V> *carry = items + kBatch * 32;
+  fv<V> *pre = carry + kMaxModes * 32;
+  uint2 *ustage = reinterpret_cast<uint2 *>(pre + kMaxModes * 32);
+  uint32_t *fstage = reinterpret_cast<uint32_t *>(ustage + kBatch);
+  uint32_t *xbuf = fstage + kBatch;
+  const int col = lane * V;
+  const bool act = col < a.R;
+  const int S = a.S, d = a.d;
+  const int top = FUSE ? S - 2 : S - 1;  // highest level whose items the level loop takes
+  const uint32_t *sc = a.sched + (size_t)chunk_id * (S + 1);
+  uint32_t nodeL = lane < S ? sc[lane] : 0u;
+  uint32_t part = sc[S];
+  uint32_t touched = 0;
+  for (int l = d; l < top; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
+  if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
+  const RowSrc<V, FT> Us(a.U_src, a.ldr, col);
+  const RowSrc<V, FT> Uf(a.U[FUSE ? S - 1 : 0], a.ldr, col);
+  fv<V> acc = fv_fill<V>(0.f);   // open node of level S-1
+  fv<V> acc2 = fv_fill<V>(0.f);  // open node of level S-2 (FUSE)
+  constexpr int SB = 16 / V;     // unit rows in flight per lane
+  constexpr int SI = 4;          // item rows in flight per lane
+  const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
+  const uint64_t u1 = min(u0 + a.chunk, a.nunits);
+  for (uint64_t base = u0; base < u1; base += kBatch) {
+    const int cnt = (int)min((uint64_t)kBatch, u1 - base);
+    const bool in = lane < cnt;
+    const uint32_t id = in ? __ldg(a.src_ids + base + lane) : 0u;
+    float v = 0.f;
+    if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
+    const uint32_t cd = in ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
+    const uint32_t M = __ballot_sync(~0u, cd >= 1u);
+    const uint32_t M2 = FUSE ? __ballot_sync(~0u, cd >= 2u) : 0u;
+    const int n1 = __popc(M);
+    ustage[lane] = make_uint2(id, __float_as_uint(v));
+    if constexpr (FUSE) {
+      const uint32_t first1 = __shfl_sync(~0u, nodeL, S - 1);
+      fstage[lane] = (lane < n1 && (uint64_t)first1 + lane < a.nfibs[S - 1])
+                         ? __ldg(a.fids[S - 1] + first1 + lane) : 0u;
+    }
+    __syncwarp();
+    int j = 0;
+    auto run = [&](auto full) {
+      constexpr bool FULL = decltype(full)::value;
+#pragma unroll
+      for (int k0 = 0; k0 < kBatch; k0 += SB) {
+        if (!FULL && k0 >= cnt) break;
+        fv<V> g[SB];
+        fv<V> r[FUSE ? SB : 1];
+        fv<V> m[LEAF ? 1 : SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const int k = k0 + q;
+          const bool ok = act && (FULL || k < cnt);
+          g[q] = Us.load(ustage[k].x, ok);
+          if constexpr (FUSE) {
+            const bool closes = (M >> k) & 1u;
+            r[q] = Uf.load(fstage[__popc(M & ((1u << k) - 1u))], ok && closes);
+          }
+          if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok);
+        }
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const int k = k0 + q;
+          if (FULL || k < cnt) {
+            if constexpr (LEAF) fv_axpy(acc, __uint_as_float(ustage[k].y), g[q]);
+            else fv_fma(acc, m[LEAF ? 0 : q], g[q]);
+            if ((M >> k) & 1u) {
+              if constexpr (FUSE) {
+                fv_fma(acc2, acc, r[FUSE ? q : 0]);
+                if ((M2 >> k) & 1u) {
+                  items[j * 32 + lane] = acc2;
+                  acc2 = fv_fill<V>(0.f);
+                  ++j;
+                }
+              } else {
+                items[j * 32 + lane] = acc;
+                ++j;
+              }
+              acc = fv_fill<V>(0.f);
+            }
+          }
+        }
+      }
+    };
+    if (cnt == kBatch) run(std::true_type{});
+    else run(std::false_type{});
+    if ((M >> (cnt - 1)) & 1u) touched &= ~(1u << (S - 1));
+    else touched |= 1u << (S - 1);
+    int n;
+    uint32_t icd;
+    if constexpr (FUSE) {
+      // level S-1 is done within the batch: advance its node (without FUSE
+      // the level loop does this when it takes the level-(S-1) items)
+      if (lane == S - 1) nodeL += (uint32_t)n1;
+      if (n1 > 0) part &= ~(1u << (S - 1));
+      if (n1 > 0) {
+        // the last level-(S-1) close in the batch decides whether acc2 is open
+        const int lastc = 31 - __clz(M);
+        if ((M2 >> lastc) & 1u) touched &= ~(1u << (S - 2));
+        else touched |= 1u << (S - 2);
+      }
+      n = __popc(M2);
+      icd = compact_bits(M2, cd - 2u, xbuf, lane);
+    } else {
+      n = n1;
+      icd = compact_bits(M, cd - 1u, xbuf, lane);
+    }
+    // the level loop: items of level l (node sums that closed in this batch)
+    for (int l = top; l >= d && n > 0; --l) {
+      const uint32_t first = __shfl_sync(~0u, nodeL, l);
+      const bool pfirst = (part >> l) & 1u;
+      const uint32_t fid =
+          (lane < n && (uint64_t)first + lane < a.nfibs[l]) ? __ldg(a.fids[l] + first + lane) : 0u;
+      float *store = a.store[l];
+      if (store != nullptr && (uint64_t)first + n <= a.nfibs[l]) {
+        for (int i = 0; i < n; ++i) {
+          const fv<V> val = items[i * 32 + lane];
+          if (i == 0 && pfirst) red_rows<V>(store, first, a.ldr, col, val, act);
+          else st_rows<V>(store, (uint64_t)first + i, a.ldr, col, val, act);
+        }
       }
       if (l > d) {
-        const float4 r = load_row<FT>(a.U[l], a.fids[l][u.node[l]], a.ldr, col, act);
-        f4_fma(u.acc[l - 1], v, r);
-        u.touched |= 1u << (l - 1);
-      } else {
-        const uint32_t orow = a.fids[l][u.node[l]];
-        if (l == 0) {
-          if (part) atomic_f4(a.out, orow, a.ldr, col, v, act);
-          else store_f4(a.out, orow, a.ldr, col, v, act);
-        } else {
-          atomic_f4(a.out, orow, a.ldr, col, f4_mul(v, u.P[l - 1]), act);
+        const uint32_t Mp = __ballot_sync(~0u, lane < n && icd >= 1u);
+        const RowSrc<V, FT> Ul(a.U[l], a.ldr, col);
+        fv<V> cl = carry[(l - 1) * 32 + lane];
+        int jj = 0;
+        for (int i0 = 0; i0 < n; i0 += SI) {
+          fv<V> r[SI];
+#pragma unroll
+          for (int q = 0; q < SI; ++q) {
+            const int i = i0 + q;
+            r[q] = Ul.load(__shfl_sync(~0u, fid, i & 31), act && i < n);
+          }
+#pragma unroll
+          for (int q = 0; q < SI; ++q) {
+            const int i = i0 + q;
+            if (i < n) {
+              fv_fma(cl, items[i * 32 + lane], r[q]);
+              if ((Mp >> i) & 1u) {
+                items[jj * 32 + lane] = cl;
+                cl = fv_fill<V>(0.f);
+                ++jj;
+              }
+            }
+          }
         }
+        carry[(l - 1) * 32 + lane] = cl;
+        if ((Mp >> (n - 1)) & 1u) touched &= ~(1u << (l - 1));
+        else touched |= 1u << (l - 1);
+        if (lane == l) nodeL += (uint32_t)n;
+        part &= ~(1u << l);
+        icd = compact_bits(Mp, icd - 1u, xbuf, lane);
+        n = __popc(Mp);
+      } else {
+        for (int i = 0; i < n; ++i) {
+          const fv<V> val = items[i * 32 + lane];
+          const uint32_t orow = __shfl_sync(~0u, fid, i);
+          if (d == 0) {
+            if (i == 0 && pfirst) red_rows<V>(a.out, orow, a.ldr, col, val, act);
+            else st_rows<V>(a.out, orow, a.ldr, col, val, act);
+          } else {
+            red_rows<V>(a.out, orow, a.ldr, col, fv_mul(val, pre[(d - 1) * 32 + lane]), act);
+            const uint32_t ci = __shfl_sync(~0u, icd, i);
+            if (ci >= 1u) nodeL = advance_prefix<V, FT>(a, pre, nodeL, d - (int)ci, d, col, act, lane);
+          }
+        }
+        if (lane == l) nodeL += (uint32_t)n;
+        part &= ~(1u << l);
+        n = 0;
       }
-      u.acc[l] = f4_zero();
-      u.touched &= ~(1u << l);
-      u.part &= ~(1u << l);
-    } else {
-      pchange = l;
     }
-    u.node[l] += 1;
-    if ((uint64_t)u.node[l] < a.nfibs[l]) u.endc[l] = a.fptr[l][u.node[l] + 1];
-    carry = l > 0 && u.node[l] == u.endc[l - 1];
   }
-  if (pchange < kMaxModes && (uint64_t)u.node[0] < a.nfibs[0])
-    upper_prefix<FT>(a, u, pchange, min(d, a.S - 1), col, act);
-}
-
-// Chunk end: the open nodes of levels d..S-2 get their partial sums added.
-template <FactorType FT>
-__device__ __noinline__ void upper_flush(const WalkArgs &a, Upper &u, float4 accP, bool touchP,
-                                         int col, bool act) {
-  const int d = a.d;
-  const int p = a.S - 2;
-  if (p >= d && touchP) {
-    u.acc[p] = accP;
-    u.touched |= 1u << p;
-  }
-  for (int l = p; l >= d; --l) {
-    if (!((u.touched >> l) & 1u)) continue;
-    const float4 v = u.acc[l];
-    if (a.store[l] != nullptr) atomic_f4(a.store[l], u.node[l], a.ldr, col, v, act);
+  // chunk end: the open nodes of levels S-1 .. d add their partial sums;
+  // the register carries first, then the shared-memory ones
+  carry[(S - 1) * 32 + lane] = acc;
+  if (FUSE) carry[(S - 2) * 32 + lane] = acc2;
+  for (int l = S - 1; l >= d; --l) {
+    if (!((touched >> l) & 1u)) continue;
+    const uint32_t node = __shfl_sync(~0u, nodeL, l);
+    if ((uint64_t)node >= a.nfibs[l]) continue;
+    const fv<V> val = carry[l * 32 + lane];
+    if (a.store[l] != nullptr) red_rows<V>(a.store[l], node, a.ldr, col, val, act);
     if (l > d) {
-      const float4 r = load_row<FT>(a.U[l], a.fids[l][u.node[l]], a.ldr, col, act);
-      f4_fma(u.acc[l - 1], v, r);
-      u.touched |= 1u << (l - 1);
+      const fv<V> r = ld_factor<V, FT>(a.U[l], __ldg(a.fids[l] + node), a.ldr, col, act);
+      fv<V> c2 = carry[(l - 1) * 32 + lane];
+      fv_fma(c2, val, r);
+      carry[(l - 1) * 32 + lane] = c2;
+      touched |= 1u << (l - 1);
     } else {
-      const uint32_t orow = a.fids[l][u.node[l]];
-      atomic_f4(a.out, orow, a.ldr, col, l == 0 ? v : f4_mul(v, u.P[l - 1]), act);
+      const uint32_t orow = __ldg(a.fids[d] + node);
+      red_rows<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
+                  act);
     }
   }
 }
 
-// Stage one batch: unit ids/values and the parent window into meta, then
-// the unit products (or memo rows) into cbuf and the window's factor rows
-// into fbuf. Returns with the group fenced.
-template <int LANES, FactorType FT, bool LEAF, bool CONTRIB>
-__device__ __forceinline__ void issue_batch(const WalkArgs &a, uint64_t base, int cnt, int t,
-                                            int col, bool act, unsigned gmask, uint32_t nodeS,
-                                            uint64_t FS, bool want_rows, float4 *cbuf,
-                                            float4 *fbuf, GroupMeta *meta) {
-  constexpr int B = kBatch;
-  for (int k = t; k < B; k += LANES) {
-    uint32_t id = 0;
+// ---------------------------------------------------------------------------
+// Scatter (S == d): every unit adds src(u) * P_{d-1} to output row
+// fids[d][u], with P_{d-1} = Q * U_{d-1}[parent] and Q the prefix of the
+// levels above the parent (it changes only where a unit closes two or more
+// levels). Units are independent, so a warp takes 32 / W of them per step:
+// W lanes per unit, 4 columns (one float4) per lane, vector atomics.
+// ---------------------------------------------------------------------------
+template <int W>
+constexpr size_t scatter_warp_smem() {
+  return (size_t)kMaxModes * 128 * sizeof(float) + kBatch * (sizeof(uint2) + sizeof(uint32_t));
+}
+template <int W>
+constexpr size_t scatter_smem() {
+  return (size_t)kWarps * scatter_warp_smem<W>();
+}
+
+template <FactorType FT>
+__device__ __forceinline__ float4 ld_factor4(const void *U, uint32_t row, int ldr, int col, bool act) {
+  const fv<4> r = ld_factor<4, FT>(U, row, ldr, col, act);
+  return make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
+}
+
+// Prefix rows (per column, all ldr columns) of levels lo..hi-1.
+template <FactorType FT>
+__device__ __noinline__ void scatter_prefix(const WalkArgs &a, float *preq, uint32_t nodeL, int lo,
+                                            int hi, int lane) {
+  const int c = 4 * lane;
+  const bool act = c < a.ldr;
+  for (int l = lo; l < hi; ++l) {
+    const uint32_t n = __shfl_sync(~0u, nodeL, l);
+    const bool valid = (uint64_t)n < a.nfibs[l];
+    const uint32_t f = valid ? __ldg(a.fids[l] + n) : 0u;
+    float4 row = ld_factor4<FT>(a.U[l], f, a.ldr, c, act && valid);
+    if (l > 0 && act) {
+      const float4 p = *reinterpret_cast<const float4 *>(preq + (l - 1) * 128 + c);
+      row = make_float4(row.x * p.x, row.y * p.y, row.z * p.z, row.w * p.w);
+    }
+    if (act) *reinterpret_cast<float4 *>(preq + l * 128 + c) = row;
+  }
+}
+
+template <int W, FactorType FT, bool LEAF>
+__global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ WalkArgs a) {
+  constexpr int UPS = 32 / W;  // units per step
+  extern __shared__ __align__(16) unsigned char walk_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t chunk_id = blockIdx.x * kWarps + warp;
+  if (chunk_id >= a.nchunks) return;
+  unsigned char *wbase = walk_raw + (size_t)warp * scatter_warp_smem<W>();
+  float *preq = reinterpret_cast<float *>(wbase);  // kMaxModes x 128 columns
+  uint2 *ustage = reinterpret_cast<uint2 *>(preq + kMaxModes * 128);
+  uint32_t *pstage = reinterpret_cast<uint32_t *>(ustage + kBatch);
+  const int slot = lane / W;
+  const int col = 4 * (lane % W);
+  const bool act = col < a.R;
+  const int d = a.S;
+  const uint32_t *sc = a.sched + (size_t)chunk_id * (d + 1);
+  uint32_t nodeL = lane < d ? sc[lane] : 0u;
+  if (d >= 2) scatter_prefix<FT>(a, preq, nodeL, 0, d - 1, lane);
+  __syncwarp();
+  const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
+  const uint64_t u1 = min(u0 + a.chunk, a.nunits);
+  for (uint64_t base = u0; base < u1; base += kBatch) {
+    const int cnt = (int)min((uint64_t)kBatch, u1 - base);
+    const bool in = lane < cnt;
+    const uint32_t id = in ? __ldg(a.src_ids + base + lane) : 0u;
     float v = 0.f;
-    if (k < cnt) {
-      id = __ldg(a.src_ids + base + k);
-      if constexpr (LEAF) v = __ldg(a.vals + base + k);
-    }
-    meta->id[k] = id;
-    meta->v[k] = v;
-    const uint64_t n = (uint64_t)nodeS + k;
-    const bool in = n < FS;
-    meta->wfid[k] = in ? __ldg(a.par_fids + n) : 0u;
-    meta->wend[k] = in ? __ldg(a.par_fptr + n + 1) : 0u;
-  }
-  __syncwarp(gmask);
-#pragma unroll
-  for (int k = 0; k < B; ++k) {
-    if (k < cnt) {
-      if constexpr (CONTRIB) {
-        const float4 row = load_row<FT>(a.U_src, meta->id[k], a.ldr, col, act);
+    if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
+    const uint32_t cd = (in && d >= 1) ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
+    const uint32_t M = __ballot_sync(~0u, cd >= 1u);
+    const uint32_t M2 = __ballot_sync(~0u, cd >= 2u);
+    // factor-row ids of the parents (level d-1) of this batch's units
+    const uint32_t nodeP = d >= 1 ? __shfl_sync(~0u, nodeL, d - 1) : 0u;
+    uint32_t pf = 0;
+    if (d >= 1 && (uint64_t)nodeP + lane < a.nfibs[d - 1]) pf = __ldg(a.fids[d - 1] + nodeP + lane);
+    ustage[lane] = make_uint2(id, __float_as_uint(v));
+    pstage[lane] = pf;
+    __syncwarp();
+    int k = 0;
+    while (k < cnt) {
+      const uint32_t rest = M2 & (~0u << k);
+      const int deep = rest ? __ffs(rest) - 1 : 32;
+      const int ke = min(deep, cnt - 1);
+      float4 Q = make_float4(1.f, 1.f, 1.f, 1.f);
+      if (d >= 2 && act) Q = *reinterpret_cast<const float4 *>(preq + (d - 2) * 128 + col);
+      for (int k0 = k; k0 <= ke; k0 += UPS) {
+        const int unit = k0 + slot;
+        const bool ok = unit <= ke && act;
+        const uint2 e = ustage[unit & 31];
+        float4 p = make_float4(1.f, 1.f, 1.f, 1.f);
+        if (d >= 1) {
+          const uint32_t f = pstage[__popc(M & ((1u << (unit & 31)) - 1u))];
+          const float4 r = ld_factor4<FT>(a.U[d - 1], f, a.ldr, col, ok);
+          p = make_float4(Q.x * r.x, Q.y * r.y, Q.z * r.z, Q.w * r.w);
+        }
+        float4 x;
         if constexpr (LEAF) {
-          cbuf[k * LANES + t] = f4_scale(meta->v[k], row);
+          const float s = __uint_as_float(e.y);
+          x = make_float4(s * p.x, s * p.y, s * p.z, s * p.w);
         } else {
-          cbuf[k * LANES + t] = f4_mul(load_f4(a.src_rows, base + k, a.ldr, col, act), row);
+          const fv<4> m = ld_rows<4>(a.src_rows, base + (unit & 31), a.ldr, col, ok);
+          x = make_float4(m.x[0] * p.x, m.x[1] * p.y, m.x[2] * p.z, m.x[3] * p.w);
         }
-      } else if constexpr (!LEAF) {
-        cbuf[k * LANES + t] = load_f4(a.src_rows, base + k, a.ldr, col, act);
+        if (ok) atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)e.x * a.ldr + col), x);
       }
+      if (deep == ke) {
+        // unit ke closes levels d-1 .. d-c (c >= 2): the levels above its
+        // parent move on and Q is recomputed
+        const int c = (int)__shfl_sync(~0u, cd, ke);
+        if (lane >= d - c && lane < d - 1) nodeL += 1;
+        if ((uint64_t)__shfl_sync(~0u, nodeL, d - c) < a.nfibs[d - c])
+          scatter_prefix<FT>(a, preq, nodeL, d - c, d - 1, lane);
+        __syncwarp();
+      }
+      k = ke + 1;
     }
-  }
-  if (want_rows) {
-#pragma unroll
-    for (int k = 0; k < B; ++k)
-      if ((uint64_t)nodeS + k < FS)
-        fbuf[k * LANES + t] = load_row<FT>(a.U_par, meta->wfid[k], a.ldr, col, act);
-  }
-}
-
-template <int LANES, FactorType FT, bool LEAF>
-__global__ void __launch_bounds__(256) k_contract(const __grid_constant__ WalkArgs a) {
-  constexpr int B = kBatch;
-  extern __shared__ float4 wsm[];
-  const uint32_t chunk_id = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;
-  if (chunk_id >= a.nchunks) return;
-  const int t = threadIdx.x % LANES;
-  const int grp = threadIdx.x / LANES;
-  float4 *cbuf = wsm + (size_t)grp * 2 * B * LANES;
-  float4 *fbuf = cbuf + B * LANES;
-  GroupMeta *meta = reinterpret_cast<GroupMeta *>(wsm + (size_t)(256 / LANES) * 2 * B * LANES) + grp;
-  const int col = 4 * t;
-  const bool act = col < a.R;
-  const unsigned gmask =
-      LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << ((threadIdx.x & 31) / LANES * LANES));
-  const int d = a.d, L1 = a.S - 1;
-  const uint32_t *sc = a.sched + (size_t)chunk_id * (a.S + 1);
-  Upper u;
-  upper_init<FT>(a, u, sc, col, act);
-  const uint64_t FS = a.par_n;
-  uint32_t nodeS = sc[L1];
-  uint32_t endS = a.par_fptr[nodeS + 1];
-  bool partS = (sc[a.S] >> L1) & 1u;
-  uint32_t endP = L1 > 0 ? u.endc[L1 - 1] : 0xffffffffu;
-  float4 pv = (L1 == d && d > 0) ? u.P[d - 1] : f4_zero();
-  float4 accS = f4_zero(), accP = f4_zero();
-  bool touchS = false, touchP = false;
-  int w = 0;
-  uint32_t open_fid = 0;  // id of the open parent node at the chunk end
-  const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
-  const uint64_t u1 = min(u0 + a.chunk, a.nunits);
-  for (uint64_t base = u0; base < u1; base += B) {
-    const int cnt = (int)min((uint64_t)B, u1 - base);
-    issue_batch<LANES, FT, LEAF, true>(a, base, cnt, t, col, act, gmask, nodeS, FS, L1 > d, cbuf,
-                                       fbuf, meta);
-    w = 0;
-    for (int k = 0; k < cnt; ++k) {
-      f4_add(accS, cbuf[k * LANES + t]);
-      touchS = true;
-      if (base + k + 1 != (uint64_t)endS) continue;
-      // the parent (level S-1) node is complete
-      const float4 val = accS;
-      accS = f4_zero();
-      touchS = false;
-      const bool was_part = partS;
-      partS = false;
-      if (a.par_store != nullptr) {
-        if (was_part) atomic_f4(a.par_store, nodeS, a.ldr, col, val, act);
-        else store_f4(a.par_store, nodeS, a.ldr, col, val, act);
-      }
-      if (L1 > d) {
-        f4_fma(accP, val, fbuf[w * LANES + t]);
-        touchP = true;
-      } else {
-        const uint32_t orow = meta->wfid[w];
-        if (d == 0) {
-          if (was_part) atomic_f4(a.out, orow, a.ldr, col, val, act);
-          else store_f4(a.out, orow, a.ldr, col, val, act);
-        } else {
-          atomic_f4(a.out, orow, a.ldr, col, f4_mul(val, pv), act);
-        }
-      }
-      ++w;
-      ++nodeS;
-      if (w < B) endS = meta->wend[w];
-      else if ((uint64_t)nodeS < FS) endS = __ldg(a.par_fptr + nodeS + 1);
-      if (L1 > 0 && nodeS == endP) {
-        upper_complete<FT>(a, u, accP, col, act);
-        accP = f4_zero();
-        touchP = false;
-        endP = u.endc[L1 - 1];
-        if (L1 == d && d > 0) pv = u.P[d - 1];
-      }
-    }
-    if (touchS) open_fid = meta->wfid[w < B ? w : B - 1];
-    __syncwarp(gmask);
-  }
-  if (touchS) {
-    if (a.par_store != nullptr) atomic_f4(a.par_store, nodeS, a.ldr, col, accS, act);
-    if (L1 > d) {
-      // the open parent node is window entry w of the last batch (w < B: it has units)
-      f4_fma(accP, accS, fbuf[w * LANES + t]);
-      touchP = true;
-    } else {
-      atomic_f4(a.out, open_fid, a.ldr, col, d == 0 ? accS : f4_mul(accS, pv), act);
-    }
-  }
-  if (L1 - 1 >= d) upper_flush<FT>(a, u, accP, touchP, col, act);
-}
-
-template <int LANES, FactorType FT, bool LEAF>
-__global__ void __launch_bounds__(256) k_scatter(const __grid_constant__ WalkArgs a) {
-  constexpr int B = kBatch;
-  extern __shared__ float4 wsm[];
-  const uint32_t chunk_id = (blockIdx.x * blockDim.x + threadIdx.x) / LANES;
-  if (chunk_id >= a.nchunks) return;
-  const int t = threadIdx.x % LANES;
-  const int grp = threadIdx.x / LANES;
-  float4 *cbuf = wsm + (size_t)grp * 2 * B * LANES;
-  float4 *fbuf = cbuf + B * LANES;
-  GroupMeta *meta = reinterpret_cast<GroupMeta *>(wsm + (size_t)(256 / LANES) * 2 * B * LANES) + grp;
-  const int col = 4 * t;
-  const bool act = col < a.R;
-  const unsigned gmask =
-      LANES == 32 ? 0xffffffffu : (((1u << LANES) - 1u) << ((threadIdx.x & 31) / LANES * LANES));
-  const int L1 = a.S - 1;  // parent level of the units; the output level is S
-  const uint32_t *sc = a.sched + (size_t)chunk_id * (a.S + 1);
-  Upper u;
-  upper_init<FT>(a, u, sc, col, act);
-  const uint64_t FS = a.par_n;
-  uint32_t nodeS = sc[L1];
-  uint32_t endS = a.par_fptr[nodeS + 1];
-  uint32_t endP = L1 > 0 ? u.endc[L1 - 1] : 0xffffffffu;
-  float4 above = L1 > 0 ? u.P[L1 - 1] : make_float4(1.f, 1.f, 1.f, 1.f);
-  const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
-  const uint64_t u1 = min(u0 + a.chunk, a.nunits);
-  for (uint64_t base = u0; base < u1; base += B) {
-    const int cnt = (int)min((uint64_t)B, u1 - base);
-    issue_batch<LANES, FT, LEAF, false>(a, base, cnt, t, col, act, gmask, nodeS, FS, true, cbuf,
-                                        fbuf, meta);
-    int w = 0;
-    float4 pv = f4_mul(above, fbuf[t]);
-    for (int k = 0; k < cnt; ++k) {
-      float4 c;
-      if constexpr (LEAF) c = f4_scale(meta->v[k], pv);
-      else c = f4_mul(cbuf[k * LANES + t], pv);
-      atomic_f4(a.out, meta->id[k], a.ldr, col, c, act);
-      if (base + k + 1 != (uint64_t)endS) continue;
-      ++w;
-      ++nodeS;
-      if (w < B) endS = meta->wend[w];
-      else if ((uint64_t)nodeS < FS) endS = __ldg(a.par_fptr + nodeS + 1);
-      if (L1 > 0 && nodeS == endP) {
-        upper_complete<FT>(a, u, f4_zero(), col, act);
-        endP = u.endc[L1 - 1];
-        above = u.P[L1 - 1];
-      }
-      if (w < B) pv = f4_mul(above, fbuf[w * LANES + t]);
-    }
-    __syncwarp(gmask);
+    if (d >= 1 && lane == d - 1) nodeL += (uint32_t)__popc(M);
+    __syncwarp();
   }
 }
 
@@ -458,39 +674,51 @@ WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   a.vals = c.vals32.get();
   a.src_rows = w.src_rows;
   a.src_ids = c.fids[w.src].get();
-  a.out_ids = c.fids[w.out].get();
+  a.src_cd = w.src >= 1 ? c.cdepth[w.src].get() : nullptr;
   a.U_src = f ? f->U[w.src] : nullptr;
-  const int par = w.src > 0 ? w.src - 1 : 0;
-  a.par_fptr = c.fptr[par].get();
-  a.par_fids = c.fids[par].get();
-  a.U_par = f ? f->U[par] : nullptr;
-  a.par_store = w.store[par];
-  a.par_n = c.nfibs[par];
   a.out = out;
   a.sched = w.sched.get();
   return a;
 }
 
-template <FactorType FT, bool LEAF, bool CONTRACT>
-void launch_lanes(int lanes, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
-#define ADATM_WALK_CASE(L)                                                \
-  case L:                                                                 \
-    if (CONTRACT)                                                         \
-      k_contract<L, FT, LEAF><<<blocks, 256, walk_smem<L>(), s>>>(a); \
-    else                                                                  \
-      k_scatter<L, FT, LEAF><<<blocks, 256, walk_smem<L>(), s>>>(a);     \
-    break;
-  switch (lanes) {
-    ADATM_WALK_CASE(4)
-    ADATM_WALK_CASE(8)
-    ADATM_WALK_CASE(16)
-    ADATM_WALK_CASE(32)
-    default: throw BadInput("unsupported lane count");
+template <FactorType FT, bool LEAF, bool FUSE>
+void launch_contract(int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+  switch (vec) {
+    case 1: k_contract<1, FT, LEAF, FUSE><<<blocks, 256, contract_smem<1>(), s>>>(a); break;
+    case 2: k_contract<2, FT, LEAF, FUSE><<<blocks, 256, contract_smem<2>(), s>>>(a); break;
+    case 4: k_contract<4, FT, LEAF, FUSE><<<blocks, 256, contract_smem<4>(), s>>>(a); break;
+    default: throw BadInput("unsupported columns per lane");
   }
-#undef ADATM_WALK_CASE
   ADATM_LAUNCH();
 }
 
+template <FactorType FT, bool LEAF>
+void launch_contract(bool fuse, int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+  if (fuse) launch_contract<FT, LEAF, true>(vec, a, blocks, s);
+  else launch_contract<FT, LEAF, false>(vec, a, blocks, s);
+}
+
+template <FactorType FT, bool LEAF>
+void launch_scatter(int w, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+  switch (w) {
+    case 4: k_scatter<4, FT, LEAF><<<blocks, 256, scatter_smem<4>(), s>>>(a); break;
+    case 8: k_scatter<8, FT, LEAF><<<blocks, 256, scatter_smem<8>(), s>>>(a); break;
+    case 16: k_scatter<16, FT, LEAF><<<blocks, 256, scatter_smem<16>(), s>>>(a); break;
+    case 32: k_scatter<32, FT, LEAF><<<blocks, 256, scatter_smem<32>(), s>>>(a); break;
+    default: throw BadInput("unsupported lanes per unit");
+  }
+  ADATM_LAUNCH();
+}
+
+// Contraction: columns per lane (32 lanes cover R).
+int vec_for_rank(int R) {
+  if (R <= 32) return 1;
+  if (R <= 64) return 2;
+  if (R <= 128) return 4;
+  throw BadInput("rank above 128 is not supported by the GPU kernels");
+}
+
+// Scatter: lanes per unit (4 columns per lane).
 int lanes_for_rank(int R) {
   if (R <= 16) return 4;
   if (R <= 32) return 8;
@@ -504,24 +732,32 @@ int lanes_for_rank(int R) {
 void set_walk_attributes() {
   static bool done = false;
   if (done) return;
-#define ADATM_ATTR(L, FT, LEAF)                                                           \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<L, FT, LEAF>,                                \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,            \
-                                  (int)walk_smem<L>()));                                  \
-  ADATM_CUDA(cudaFuncSetAttribute(k_scatter<L, FT, LEAF>,                                 \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,            \
-                                  (int)walk_smem<L>()));
-#define ADATM_ATTR_L(L)                        \
-  ADATM_ATTR(L, FactorType::F32, true)         \
-  ADATM_ATTR(L, FactorType::F32, false)        \
-  ADATM_ATTR(L, FactorType::BF16, true)        \
-  ADATM_ATTR(L, FactorType::BF16, false)
-  ADATM_ATTR_L(4)
-  ADATM_ATTR_L(8)
-  ADATM_ATTR_L(16)
-  ADATM_ATTR_L(32)
-#undef ADATM_ATTR_L
-#undef ADATM_ATTR
+#define ADATM_ATTR_C(V, FT, LEAF)                                                 \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, true>,                  \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                  (int)contract_smem<V>()));                      \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, false>,                 \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                  (int)contract_smem<V>()));
+#define ADATM_ATTR_S(W, FT, LEAF)                                                 \
+  ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF>,                         \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                  (int)scatter_smem<W>()));
+#define ADATM_ATTR_ALL(M, X)                \
+  M(X, FactorType::F32, true)               \
+  M(X, FactorType::F32, false)              \
+  M(X, FactorType::BF16, true)              \
+  M(X, FactorType::BF16, false)
+  ADATM_ATTR_ALL(ADATM_ATTR_C, 1)
+  ADATM_ATTR_ALL(ADATM_ATTR_C, 2)
+  ADATM_ATTR_ALL(ADATM_ATTR_C, 4)
+  ADATM_ATTR_ALL(ADATM_ATTR_S, 4)
+  ADATM_ATTR_ALL(ADATM_ATTR_S, 8)
+  ADATM_ATTR_ALL(ADATM_ATTR_S, 16)
+  ADATM_ATTR_ALL(ADATM_ATTR_S, 32)
+#undef ADATM_ATTR_ALL
+#undef ADATM_ATTR_S
+#undef ADATM_ATTR_C
   done = true;
 }
 
@@ -548,20 +784,27 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
     k_prezero<<<(w.nchunks + 7) / 8, blk, 0, s>>>(a, w.sched.get());
     ADATM_LAUNCH();
   }
-  const int lanes = lanes_for_rank(w.R);
-  const unsigned blocks = (unsigned)(((uint64_t)w.nchunks * lanes + 255) / 256);
+  const unsigned blocks = (unsigned)((w.nchunks + kWarps - 1) / kWarps);
   const bool leaf = w.src == w.nmodes - 1;
-  const bool contract = w.src > w.out;
-  if (ft == FactorType::F32) {
-    if (leaf && contract) launch_lanes<FactorType::F32, true, true>(lanes, a, blocks, s);
-    else if (leaf) launch_lanes<FactorType::F32, true, false>(lanes, a, blocks, s);
-    else if (contract) launch_lanes<FactorType::F32, false, true>(lanes, a, blocks, s);
-    else launch_lanes<FactorType::F32, false, false>(lanes, a, blocks, s);
+  if (w.src > w.out) {
+    const int vec = vec_for_rank(w.R);
+    const bool fuse = w.src - 1 > w.out && w.store[w.src - 1] == nullptr;
+    if (ft == FactorType::F32) {
+      if (leaf) launch_contract<FactorType::F32, true>(fuse, vec, a, blocks, s);
+      else launch_contract<FactorType::F32, false>(fuse, vec, a, blocks, s);
+    } else {
+      if (leaf) launch_contract<FactorType::BF16, true>(fuse, vec, a, blocks, s);
+      else launch_contract<FactorType::BF16, false>(fuse, vec, a, blocks, s);
+    }
   } else {
-    if (leaf && contract) launch_lanes<FactorType::BF16, true, true>(lanes, a, blocks, s);
-    else if (leaf) launch_lanes<FactorType::BF16, true, false>(lanes, a, blocks, s);
-    else if (contract) launch_lanes<FactorType::BF16, false, true>(lanes, a, blocks, s);
-    else launch_lanes<FactorType::BF16, false, false>(lanes, a, blocks, s);
+    const int lanes = lanes_for_rank(w.R);
+    if (ft == FactorType::F32) {
+      if (leaf) launch_scatter<FactorType::F32, true>(lanes, a, blocks, s);
+      else launch_scatter<FactorType::F32, false>(lanes, a, blocks, s);
+    } else {
+      if (leaf) launch_scatter<FactorType::BF16, true>(lanes, a, blocks, s);
+      else launch_scatter<FactorType::BF16, false>(lanes, a, blocks, s);
+    }
   }
 }
 
