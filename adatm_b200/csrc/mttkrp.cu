@@ -178,15 +178,17 @@ template <int V, FactorType FT>
 struct RowSrc {
   const char *base = nullptr;
   uint32_t stride = 0;
-  __device__ __forceinline__ RowSrc(const void *U, int ldr, int col) {
+  // Lanes past the rank read column 0 (their results are never stored).
+  __device__ __forceinline__ RowSrc(const void *U, int ldr, int col, bool act) {
     constexpr int esz = FT == FactorType::F32 ? 4 : 2;
-    base = static_cast<const char *>(U) + (size_t)col * esz;
+    base = static_cast<const char *>(U) + (size_t)(act ? col : 0) * esz;
     stride = (uint32_t)ldr * esz;
   }
+  // Row `row`, or row 0 when !on: the load is always issued at a valid
+  // address, so no branch splits a batch of loads.
   __device__ __forceinline__ fv<V> load(uint32_t row, bool on) const {
-    fv<V> r = fv_fill<V>(0.f);
-    if (!on) return r;
-    const char *p = base + (size_t)row * stride;
+    fv<V> r;
+    const char *p = base + (size_t)(on ? row : 0u) * stride;
     if constexpr (FT == FactorType::F32) {
       if constexpr (V == 1) {
         r.x[0] = __ldg(reinterpret_cast<const float *>(p));
@@ -225,13 +227,12 @@ struct RowSrc {
 // Shared memory of one contraction warp: kBatch item rows, a carry row per
 // level (the open node's partial sum) and a prefix row per level (P_l = U_0
 // [node_0] * ... * U_l[node_l] for the levels above d), all in fv<V> slots of
-// 32 lanes; then the batch's (id, value) pairs, the factor-row ids of the
-// parent nodes that close in the batch, and a 32-word exchange buffer.
+// 32 lanes; then the batch's (id, value) pairs and a 32-word exchange buffer.
 constexpr int kSlots = kBatch + 2 * kMaxModes;
 
 template <int V>
 constexpr size_t contract_warp_smem() {
-  return (size_t)kSlots * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint2) + 2 * sizeof(uint32_t));
+  return (size_t)kSlots * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint2) + sizeof(uint32_t));
 }
 template <int V>
 constexpr size_t contract_smem() {
@@ -276,16 +277,19 @@ __device__ __forceinline__ uint32_t compact_bits(uint32_t m, uint32_t value, uin
 // Contraction (S > d).
 //
 // The source units of a batch are summed into the open node of level S-1
-// (carry `acc`, in registers). With FUSE (S-1 > d and no memo store at level
-// S-1), a unit that closes its level-(S-1) node also multiplies the node's sum
-// by the node's own factor row -- gathered, for the closing units only, in
-// the same batch of loads -- and adds it to the open node of level S-2 (carry
-// `acc2`, in registers); the nodes of level S-2 that close become the items
-// of the level loop. Without FUSE the closed level-(S-1) nodes are the items.
-// The level loop takes the items up one level at a time (memo stores, factor
-// rows, carries of the levels above in shared memory) until level d.
-template <int V, FactorType FT, bool LEAF, bool FUSE>
-__global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ WalkArgs a) {
+// (carry `acc`, in registers); the level-(S-1) nodes that close become the
+// batch's items. The level loop then takes the items up one level at a time
+// -- memo stores, the items' own factor rows, carries of the levels above in
+// shared memory -- until level d. Resident blocks per SM follow the shared
+// memory a block takes (4 at V = 1, so at most 64 registers per thread).
+template <int V>
+constexpr int contract_min_blocks() {
+  return V == 1 ? 4 : (V == 2 ? 2 : 1);
+}
+
+template <int V, FactorType FT, bool LEAF>
+__global__ void __launch_bounds__(256, contract_min_blocks<V>())
+    k_contract(const __grid_constant__ WalkArgs a) {
   extern __shared__ __align__(16) unsigned char walk_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t chunk_id = blockIdx.x * kWarps + warp;
@@ -295,24 +299,19 @@ __global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ Wal
   fv<V> *carry = items + kBatch * 32;
   fv<V> *pre = carry + kMaxModes * 32;
   uint2 *ustage = reinterpret_cast<uint2 *>(pre + kMaxModes * 32);
-  uint32_t *fstage = reinterpret_cast<uint32_t *>(ustage + kBatch);
-  uint32_t *xbuf = fstage + kBatch;
+  uint32_t *xbuf = reinterpret_cast<uint32_t *>(ustage + kBatch);
   const int col = lane * V;
   const bool act = col < a.R;
   const int S = a.S, d = a.d;
-  const int top = FUSE ? S - 2 : S - 1;  // highest level whose items the level loop takes
   const uint32_t *sc = a.sched + (size_t)chunk_id * (S + 1);
   uint32_t nodeL = lane < S ? sc[lane] : 0u;
   uint32_t part = sc[S];
   uint32_t touched = 0;
-  for (int l = d; l < top; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
+  for (int l = d; l < S - 1; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
   if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
-  const RowSrc<V, FT> Us(a.U_src, a.ldr, col);
-  const RowSrc<V, FT> Uf(a.U[FUSE ? S - 1 : 0], a.ldr, col);
-  fv<V> acc = fv_fill<V>(0.f);   // open node of level S-1
-  fv<V> acc2 = fv_fill<V>(0.f);  // open node of level S-2 (FUSE)
-  constexpr int SB = 16 / V;     // unit rows in flight per lane
-  constexpr int SI = 4;          // item rows in flight per lane
+  const RowSrc<V, FT> Us(a.U_src, a.ldr, col, act);
+  fv<V> acc = fv_fill<V>(0.f);  // open node of level S-1
+  constexpr int SB = 8 / V;     // unit rows in flight per lane
   const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
   const uint64_t u1 = min(u0 + a.chunk, a.nunits);
   for (uint64_t base = u0; base < u1; base += kBatch) {
@@ -323,14 +322,7 @@ __global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ Wal
     if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
     const uint32_t cd = in ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
     const uint32_t M = __ballot_sync(~0u, cd >= 1u);
-    const uint32_t M2 = FUSE ? __ballot_sync(~0u, cd >= 2u) : 0u;
-    const int n1 = __popc(M);
     ustage[lane] = make_uint2(id, __float_as_uint(v));
-    if constexpr (FUSE) {
-      const uint32_t first1 = __shfl_sync(~0u, nodeL, S - 1);
-      fstage[lane] = (lane < n1 && (uint64_t)first1 + lane < a.nfibs[S - 1])
-                         ? __ldg(a.fids[S - 1] + first1 + lane) : 0u;
-    }
     __syncwarp();
     int j = 0;
     auto run = [&](auto full) {
@@ -339,17 +331,12 @@ __global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ Wal
       for (int k0 = 0; k0 < kBatch; k0 += SB) {
         if (!FULL && k0 >= cnt) break;
         fv<V> g[SB];
-        fv<V> r[FUSE ? SB : 1];
         fv<V> m[LEAF ? 1 : SB];
 #pragma unroll
         for (int q = 0; q < SB; ++q) {
           const int k = k0 + q;
           const bool ok = act && (FULL || k < cnt);
           g[q] = Us.load(ustage[k].x, ok);
-          if constexpr (FUSE) {
-            const bool closes = (M >> k) & 1u;
-            r[q] = Uf.load(fstage[__popc(M & ((1u << k) - 1u))], ok && closes);
-          }
           if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok);
         }
 #pragma unroll
@@ -359,18 +346,9 @@ __global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ Wal
             if constexpr (LEAF) fv_axpy(acc, __uint_as_float(ustage[k].y), g[q]);
             else fv_fma(acc, m[LEAF ? 0 : q], g[q]);
             if ((M >> k) & 1u) {
-              if constexpr (FUSE) {
-                fv_fma(acc2, acc, r[FUSE ? q : 0]);
-                if ((M2 >> k) & 1u) {
-                  items[j * 32 + lane] = acc2;
-                  acc2 = fv_fill<V>(0.f);
-                  ++j;
-                }
-              } else {
-                items[j * 32 + lane] = acc;
-                ++j;
-              }
+              items[j * 32 + lane] = acc;
               acc = fv_fill<V>(0.f);
+              ++j;
             }
           }
         }
@@ -380,62 +358,37 @@ __global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ Wal
     else run(std::false_type{});
     if ((M >> (cnt - 1)) & 1u) touched &= ~(1u << (S - 1));
     else touched |= 1u << (S - 1);
-    int n;
-    uint32_t icd;
-    if constexpr (FUSE) {
-      // level S-1 is done within the batch: advance its node (without FUSE
-      // the level loop does this when it takes the level-(S-1) items)
-      if (lane == S - 1) nodeL += (uint32_t)n1;
-      if (n1 > 0) part &= ~(1u << (S - 1));
-      if (n1 > 0) {
-        // the last level-(S-1) close in the batch decides whether acc2 is open
-        const int lastc = 31 - __clz(M);
-        if ((M2 >> lastc) & 1u) touched &= ~(1u << (S - 2));
-        else touched |= 1u << (S - 2);
-      }
-      n = __popc(M2);
-      icd = compact_bits(M2, cd - 2u, xbuf, lane);
-    } else {
-      n = n1;
-      icd = compact_bits(M, cd - 1u, xbuf, lane);
-    }
+    int n = __popc(M);
+    uint32_t icd = compact_bits(M, cd - 1u, xbuf, lane);
     // the level loop: items of level l (node sums that closed in this batch)
-    for (int l = top; l >= d && n > 0; --l) {
+    for (int l = S - 1; l >= d && n > 0; --l) {
       const uint32_t first = __shfl_sync(~0u, nodeL, l);
       const bool pfirst = (part >> l) & 1u;
       const uint32_t fid =
           (lane < n && (uint64_t)first + lane < a.nfibs[l]) ? __ldg(a.fids[l] + first + lane) : 0u;
       float *store = a.store[l];
       if (store != nullptr && (uint64_t)first + n <= a.nfibs[l]) {
-        for (int i = 0; i < n; ++i) {
-          const fv<V> val = items[i * 32 + lane];
-          if (i == 0 && pfirst) red_rows<V>(store, first, a.ldr, col, val, act);
-          else st_rows<V>(store, (uint64_t)first + i, a.ldr, col, val, act);
+        float *sp = store + (size_t)first * a.ldr + col;
+        if (pfirst) red_rows<V>(sp, 0, 0, 0, items[lane], act);
+        else st_rows<V>(sp, 0, 0, 0, items[lane], act);
+        for (int i = 1; i < n; ++i) {
+          sp += a.ldr;
+          st_rows<V>(sp, 0, 0, 0, items[i * 32 + lane], act);
         }
       }
       if (l > d) {
         const uint32_t Mp = __ballot_sync(~0u, lane < n && icd >= 1u);
-        const RowSrc<V, FT> Ul(a.U[l], a.ldr, col);
+        const RowSrc<V, FT> Ul(a.U[l], a.ldr, col, act);
         fv<V> cl = carry[(l - 1) * 32 + lane];
         int jj = 0;
-        for (int i0 = 0; i0 < n; i0 += SI) {
-          fv<V> r[SI];
-#pragma unroll
-          for (int q = 0; q < SI; ++q) {
-            const int i = i0 + q;
-            r[q] = Ul.load(__shfl_sync(~0u, fid, i & 31), act && i < n);
-          }
-#pragma unroll
-          for (int q = 0; q < SI; ++q) {
-            const int i = i0 + q;
-            if (i < n) {
-              fv_fma(cl, items[i * 32 + lane], r[q]);
-              if ((Mp >> i) & 1u) {
-                items[jj * 32 + lane] = cl;
-                cl = fv_fill<V>(0.f);
-                ++jj;
-              }
-            }
+#pragma unroll 4
+        for (int i = 0; i < n; ++i) {
+          const fv<V> row = Ul.load(__shfl_sync(~0u, fid, i), true);
+          fv_fma(cl, items[i * 32 + lane], row);
+          if ((Mp >> i) & 1u) {
+            items[jj * 32 + lane] = cl;
+            cl = fv_fill<V>(0.f);
+            ++jj;
           }
         }
         carry[(l - 1) * 32 + lane] = cl;
@@ -464,10 +417,8 @@ __global__ void __launch_bounds__(256, 1) k_contract(const __grid_constant__ Wal
       }
     }
   }
-  // chunk end: the open nodes of levels S-1 .. d add their partial sums;
-  // the register carries first, then the shared-memory ones
+  // chunk end: the open nodes of levels S-1 .. d add their partial sums
   carry[(S - 1) * 32 + lane] = acc;
-  if (FUSE) carry[(S - 2) * 32 + lane] = acc2;
   for (int l = S - 1; l >= d; --l) {
     if (!((touched >> l) & 1u)) continue;
     const uint32_t node = __shfl_sync(~0u, nodeL, l);
@@ -681,21 +632,15 @@ WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   return a;
 }
 
-template <FactorType FT, bool LEAF, bool FUSE>
+template <FactorType FT, bool LEAF>
 void launch_contract(int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
   switch (vec) {
-    case 1: k_contract<1, FT, LEAF, FUSE><<<blocks, 256, contract_smem<1>(), s>>>(a); break;
-    case 2: k_contract<2, FT, LEAF, FUSE><<<blocks, 256, contract_smem<2>(), s>>>(a); break;
-    case 4: k_contract<4, FT, LEAF, FUSE><<<blocks, 256, contract_smem<4>(), s>>>(a); break;
+    case 1: k_contract<1, FT, LEAF><<<blocks, 256, contract_smem<1>(), s>>>(a); break;
+    case 2: k_contract<2, FT, LEAF><<<blocks, 256, contract_smem<2>(), s>>>(a); break;
+    case 4: k_contract<4, FT, LEAF><<<blocks, 256, contract_smem<4>(), s>>>(a); break;
     default: throw BadInput("unsupported columns per lane");
   }
   ADATM_LAUNCH();
-}
-
-template <FactorType FT, bool LEAF>
-void launch_contract(bool fuse, int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
-  if (fuse) launch_contract<FT, LEAF, true>(vec, a, blocks, s);
-  else launch_contract<FT, LEAF, false>(vec, a, blocks, s);
 }
 
 template <FactorType FT, bool LEAF>
@@ -733,10 +678,7 @@ void set_walk_attributes() {
   static bool done = false;
   if (done) return;
 #define ADATM_ATTR_C(V, FT, LEAF)                                                 \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, true>,                  \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                  (int)contract_smem<V>()));                      \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, false>,                 \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF>,                        \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)contract_smem<V>()));
 #define ADATM_ATTR_S(W, FT, LEAF)                                                 \
@@ -788,13 +730,12 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
   const bool leaf = w.src == w.nmodes - 1;
   if (w.src > w.out) {
     const int vec = vec_for_rank(w.R);
-    const bool fuse = w.src - 1 > w.out && w.store[w.src - 1] == nullptr;
     if (ft == FactorType::F32) {
-      if (leaf) launch_contract<FactorType::F32, true>(fuse, vec, a, blocks, s);
-      else launch_contract<FactorType::F32, false>(fuse, vec, a, blocks, s);
+      if (leaf) launch_contract<FactorType::F32, true>(vec, a, blocks, s);
+      else launch_contract<FactorType::F32, false>(vec, a, blocks, s);
     } else {
-      if (leaf) launch_contract<FactorType::BF16, true>(fuse, vec, a, blocks, s);
-      else launch_contract<FactorType::BF16, false>(fuse, vec, a, blocks, s);
+      if (leaf) launch_contract<FactorType::BF16, true>(vec, a, blocks, s);
+      else launch_contract<FactorType::BF16, false>(vec, a, blocks, s);
     }
   } else {
     const int lanes = lanes_for_rank(w.R);
