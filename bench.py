@@ -121,7 +121,9 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """One process per GPU from torchrun's environment. The backend is NCCL
+    when CUDA is present (gloo otherwise, which the CPU tests use)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -130,18 +132,25 @@ def dist_setup():
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
 def max_over_ranks(x, world):
+    """Maximum of a per-rank scalar (the device time of the timed region)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -150,6 +159,12 @@ def barrier(world):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def replica_ms_per_sweep(ms_total_max, steps, world):
+    """Whole-job ms per sweep for `world` independent replicas that each ran
+    `steps` sweeps in ms_total_max (the slowest rank's time)."""
+    return ms_total_max / (steps * world)
 
 
 # ---------------------------------------------------------------------------
@@ -355,7 +370,8 @@ def run_ours(args):
     if rank != 0:
         return 0
     line = {
-        "metric": METRIC, "value": ms_total / (K * world), "unit": "ms/sweep", "n_gpus": world,
+        "metric": METRIC, "value": replica_ms_per_sweep(ms_total, K, world), "unit": "ms/sweep",
+        "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": ms_step, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded device generator with the workload's shapes and distributions)",
