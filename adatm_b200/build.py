@@ -53,9 +53,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    _build_cli(force)
     if verbose:
         print(LIB)
     return LIB
+
+
+CLI_SRC = os.path.join(HERE, "cli", "splatt_cli.c")
+CLI = os.path.join(HERE, "splatt")
+
+
+def _build_cli(force: bool = False) -> str:
+    """The `splatt` command (cpd, bench -a adatm), linked to the library with
+    an $ORIGIN run path so it finds libadatm_b200.so beside itself."""
+    if (not force and os.path.exists(CLI) and os.path.getmtime(CLI) >= os.path.getmtime(CLI_SRC)
+            and os.path.getmtime(CLI) >= os.path.getmtime(LIB)):
+        return CLI
+    cmd = ["gcc", "-O2", "-std=gnu99", "-Wall", "-I", os.path.join(ROOT, "include"), CLI_SRC,
+           "-o", CLI, "-L", HERE, "-ladatm_b200", "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"building the splatt command failed:\n{r.stdout}\n{r.stderr}")
+    return CLI
 
 
 if __name__ == "__main__":

@@ -1,7 +1,7 @@
 """Run CP-ALS sweeps on a seeded synthetic tensor (for profilers).
 
     python -m adatm_b200.profile_case [--nnz 8000000] [--sweeps 3] [--dims 5000,5000,2000,500]
-                                      [--alpha 1.1] [--rank 32] [--bf16] [--plain]
+                                      [--alpha 1.1] [--rank 32] [--bf16] [--plain] [--lognormal]
 
 Builds the tensor, the analytic plan (or the plain one-tree-per-mode plan with
 --plain) and the engine on device 0, then runs the given number of sweeps
@@ -23,10 +23,11 @@ def main():
     ap.add_argument("--plain", action="store_true")
     ap.add_argument("--time", action="store_true", help="print per-mode MTTKRP and sweep times")
     ap.add_argument("--chunk", type=int, default=0, help="source units per chunk (0 = default)")
+    ap.add_argument("--lognormal", action="store_true", help="values lognormal(0, 1) instead of U(0, 1)")
     a = ap.parse_args()
     dims = [int(x) for x in a.dims.split(",")]
     A.lib().adatm_set_device(0)
-    t = A.Tensor.generate(dims, a.nnz, alpha=a.alpha, seed=0)
+    t = A.Tensor.generate(dims, a.nnz, alpha=a.alpha, value_kind=1 if a.lognormal else 0, seed=0)
     plan = A.plan_splatt(t, A.CSF_ALLMODE) if a.plain else A.plan_analytic(t, a.rank)[0]
     e = A.Engine(t, a.rank, plan, bf16=a.bf16, chunk_leaf=a.chunk, chunk_rows=a.chunk)
     e.init_factors(0)
