@@ -446,6 +446,138 @@ def plan_splatt(tensor: Tensor, csf_alloc):
     return _plan_to_py(p)
 
 
+# ---------------------------------------------------------------------------
+# Learned plan model
+# ---------------------------------------------------------------------------
+
+PLAN_FEATURES = 16
+
+
+def plan_features(tensor: Tensor, rank):
+    """Candidate plans of decide_candidate_configs with their features
+    (ncand x PLAN_FEATURES, float32) and exact device bytes."""
+    X = np.zeros((64, PLAN_FEATURES), dtype=np.float32)
+    b = np.zeros(64)
+    cands = (AdatmCandidate * 64)()
+    nc = C.c_int(0)
+    rc = lib().adatm_plan_features(tensor._h, rank, X.ctypes.data_as(C.POINTER(C.c_float)),
+                                   b.ctypes.data_as(C.POINTER(C.c_double)), cands, 64, C.byref(nc))
+    _check(rc, "adatm_plan_features")
+    n = min(nc.value, 64)
+    cl = [dict(_plan_to_py(cands[i].plan), pspace=int(cands[i].pspace), pops=int(cands[i].pops))
+          for i in range(n)]
+    return X[:n].copy(), b[:n].copy(), cl
+
+
+def _f32(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """The plan model's network on the GPU (forward, gradient and Adam
+    training by the library's own kernels)."""
+
+    def __init__(self, widths, seed=0):
+        w = (C.c_int * len(widths))(*widths)
+        h = C.c_void_p()
+        _check(lib().adatm_mlp_create(len(widths), w, seed, C.byref(h)), "adatm_mlp_create")
+        self._h = h
+        self.widths = list(widths)
+        n = C.c_uint64(0)
+        _check(lib().adatm_mlp_nparams(h, C.byref(n)), "adatm_mlp_nparams")
+        self.nparams = n.value
+
+    def get_params(self):
+        out = np.zeros(self.nparams, dtype=np.float32)
+        _check(lib().adatm_mlp_get_params(self._h, out.ctypes.data_as(C.POINTER(C.c_float))),
+               "adatm_mlp_get_params")
+        return out
+
+    def set_params(self, params):
+        a, p = _f32(params)
+        assert a.size == self.nparams
+        _check(lib().adatm_mlp_set_params(self._h, p), "adatm_mlp_set_params")
+
+    def forward(self, X):
+        a, p = _f32(X)
+        y = np.zeros(a.shape[0], dtype=np.float32)
+        _check(lib().adatm_mlp_forward(self._h, p, a.shape[0], y.ctypes.data_as(C.POINTER(C.c_float))),
+               "adatm_mlp_forward")
+        return y
+
+    def gradient(self, X, T):
+        a, p = _f32(X)
+        t, tp = _f32(T)
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = C.c_double(0)
+        _check(lib().adatm_mlp_gradient(self._h, p, tp, a.shape[0], g.ctypes.data_as(C.POINTER(C.c_float)),
+                                        C.byref(loss)), "adatm_mlp_gradient")
+        return loss.value, g
+
+    def train(self, X, T, epochs, batch, lr, seed=0):
+        a, p = _f32(X)
+        t, tp = _f32(T)
+        loss = C.c_double(0)
+        _check(lib().adatm_mlp_train(self._h, p, tp, a.shape[0], epochs, batch, lr, seed,
+                                     C.byref(loss)), "adatm_mlp_train")
+        return loss.value
+
+    def free(self):
+        if self._h:
+            lib().adatm_mlp_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class PlanModel:
+    """A trained plan model: network widths and parameters plus the feature
+    standardisation, stored as one .npz."""
+
+    def __init__(self, widths, params, mean, std):
+        self.widths = [int(w) for w in widths]
+        self.mean = np.ascontiguousarray(mean, dtype=np.float32)
+        self.std = np.ascontiguousarray(std, dtype=np.float32)
+        self.net = Mlp(self.widths)
+        self.net.set_params(params)
+
+    @classmethod
+    def load(cls, path):
+        z = np.load(path)
+        return cls(z["widths"], z["params"], z["mean"], z["std"])
+
+    def save(self, path, **extra):
+        np.savez(path, widths=np.array(self.widths), params=self.net.get_params(), mean=self.mean,
+                 std=self.std, **extra)
+
+    def predict(self, X):
+        return self.net.forward((np.asarray(X, dtype=np.float32) - self.mean) / self.std)
+
+
+def plan_learned(tensor: Tensor, rank, model: PlanModel | None):
+    """The learned plan (lowest predicted sweep time within the storage
+    limit); the analytic plan when model is None. Returns (plan, chosen
+    candidate index, whether the model decided)."""
+    p = AdatmPlan()
+    ch = C.c_int(0)
+    used = C.c_int(0)
+    if model is None:
+        rc = lib().adatm_plan_learned(tensor._h, rank, None, None, None, C.byref(p), C.byref(ch),
+                                      C.byref(used))
+    else:
+        rc = lib().adatm_plan_learned(tensor._h, rank, model.net._h,
+                                      model.mean.ctypes.data_as(C.POINTER(C.c_float)),
+                                      model.std.ctypes.data_as(C.POINTER(C.c_float)), C.byref(p),
+                                      C.byref(ch), C.byref(used))
+    _check(rc, "adatm_plan_learned")
+    return _plan_to_py(p), ch.value, bool(used.value)
+
+
 class Engine:
     """Trees, memo rows and factors of one plan and rank, resident in HBM."""
 

@@ -148,6 +148,21 @@ _SIGS = [
     ("adatm_engine_time_mttkrp", C.c_int, [C.c_void_p, u64, C.c_int, C.POINTER(C.c_float)]),
     ("adatm_engine_fit", C.c_int, [C.c_void_p, P_f64]),
     ("adatm_engine_mttkrp_bytes", C.c_int, [C.c_void_p, u64, P_f64]),
+    ("adatm_plan_features", C.c_int, [C.c_void_p, u64, C.POINTER(C.c_float), P_f64,
+                                      C.POINTER(AdatmCandidate), C.c_int, C.POINTER(C.c_int)]),
+    ("adatm_mlp_create", C.c_int, [C.c_int, C.POINTER(C.c_int), u64, C.POINTER(C.c_void_p)]),
+    ("adatm_mlp_free", None, [C.c_void_p]),
+    ("adatm_mlp_nparams", C.c_int, [C.c_void_p, P_u64]),
+    ("adatm_mlp_set_params", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    ("adatm_mlp_get_params", C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    ("adatm_mlp_forward", C.c_int, [C.c_void_p, C.POINTER(C.c_float), u64, C.POINTER(C.c_float)]),
+    ("adatm_mlp_gradient", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), u64,
+                                     C.POINTER(C.c_float), P_f64]),
+    ("adatm_mlp_train", C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), u64,
+                                  C.c_int, C.c_int, C.c_float, u64, P_f64]),
+    ("adatm_plan_learned", C.c_int, [C.c_void_p, u64, C.c_void_p, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float), C.POINTER(AdatmPlan), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int)]),
     ("adatm_gram", C.c_int, [C.c_void_p, u64, C.c_int, C.c_int, C.c_void_p]),
     ("adatm_gram_noalloc", C.c_int, [C.c_void_p, u64, C.c_int, C.c_int, C.c_void_p, C.c_void_p]),
     ("adatm_engine_launch_counts", C.c_int, [C.c_void_p, u64, C.POINTER(C.c_int), C.POINTER(C.c_int)]),

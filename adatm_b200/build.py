@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
                 "-I", os.path.join(ROOT, "include"), "-I", CSRC, "--expt-relaxed-constexpr",
                 "-ccbin", "/usr/bin/g++"]
-SOURCES = ["scan.cu", "csf_build.cu", "mttkrp.cu", "als.cu", "engine.cu", "planner.cpp", "api.cu"]
+SOURCES = ["scan.cu", "csf_build.cu", "mttkrp.cu", "als.cu", "mlp.cu", "engine.cu", "planner.cpp", "api.cu"]
 
 
 def _headers_mtime() -> float:

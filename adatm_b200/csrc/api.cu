@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "engine.hpp"
+#include "mlp.hpp"
 
 extern "C" {
 #include "adatm_b200.h"
@@ -312,6 +313,11 @@ std::shared_ptr<DevCoo> coo_of(sptensor_t *tt, cudaStream_t s) {
 struct adatm_tensor {
   StreamOwner stream;
   std::shared_ptr<DevCoo> coo;
+};
+
+struct adatm_mlp {
+  StreamOwner stream;
+  std::unique_ptr<Mlp> net;
 };
 
 struct adatm_engine {
@@ -1137,6 +1143,110 @@ int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes) {
   return guarded([&] {
     if (mode >= (uint64_t)e->eng->nmodes()) throw BadInput("mode out of range");
     *bytes = e->eng->mttkrp_bytes((int)mode);
+  });
+}
+
+int adatm_plan_features(const adatm_tensor *t, uint64_t rank, float *features, double *bytes,
+                        adatm_candidate *cands, int max_cands, int *ncands) {
+  return guarded([&] {
+    if (!t || rank < 1) throw BadInput("adatm_plan_features: no tensor or rank 0");
+    std::vector<Candidate> all = candidate_configs(t->coo->nmodes, t->coo->dims);
+    predict_candidates(*t->coo, rank, all, t->stream.s);
+    std::vector<float> f;
+    std::vector<double> b;
+    plan_features(*t->coo, rank, all, f, b, t->stream.s);
+    if (ncands) *ncands = (int)all.size();
+    for (int i = 0; i < (int)all.size() && i < max_cands; ++i) {
+      if (features) memcpy(features + (size_t)i * kPlanFeatures, &f[(size_t)i * kPlanFeatures],
+                           kPlanFeatures * sizeof(float));
+      if (bytes) bytes[i] = b[i];
+      if (cands) {
+        Plan q = all[i].plan;
+        decide_use_csfs(q);
+        plan_to_c(q, &cands[i].plan);
+        cands[i].pspace = all[i].pspace;
+        cands[i].pops = all[i].pops;
+      }
+    }
+  });
+}
+
+int adatm_mlp_create(int nwidths, const int *widths, uint64_t seed, adatm_mlp **out) {
+  return guarded([&] {
+    if (nwidths < 2 || !widths || !out) throw BadInput("adatm_mlp_create: bad widths");
+    auto m = std::make_unique<adatm_mlp>();
+    m->net = std::make_unique<Mlp>(std::vector<int>(widths, widths + nwidths), seed, m->stream.s);
+    *out = m.release();
+  });
+}
+
+void adatm_mlp_free(adatm_mlp *m) { delete m; }
+
+int adatm_mlp_nparams(const adatm_mlp *m, uint64_t *n) {
+  return guarded([&] { *n = m->net->nparams(); });
+}
+
+int adatm_mlp_set_params(adatm_mlp *m, const float *params) {
+  return guarded([&] { m->net->set_params(params); });
+}
+
+int adatm_mlp_get_params(const adatm_mlp *m, float *params) {
+  return guarded([&] { m->net->get_params(params); });
+}
+
+int adatm_mlp_forward(adatm_mlp *m, const float *X, uint64_t rows, float *Y) {
+  return guarded([&] {
+    if (rows > (1u << 30)) throw BadInput("adatm_mlp_forward: too many rows");
+    m->net->forward(X, (int)rows, Y);
+  });
+}
+
+int adatm_mlp_gradient(adatm_mlp *m, const float *X, const float *T, uint64_t rows, float *grad,
+                       double *loss) {
+  return guarded([&] {
+    if (rows == 0 || rows > (1u << 30)) throw BadInput("adatm_mlp_gradient: bad row count");
+    const double l = m->net->gradient(X, T, (int)rows, grad);
+    if (loss) *loss = l;
+  });
+}
+
+int adatm_mlp_train(adatm_mlp *m, const float *X, const float *T, uint64_t rows, int epochs,
+                    int batch, float lr, uint64_t seed, double *loss) {
+  return guarded([&] {
+    const double l = m->net->train(X, T, rows, epochs, batch, lr, seed);
+    if (loss) *loss = l;
+  });
+}
+
+int adatm_plan_learned(const adatm_tensor *t, uint64_t rank, adatm_mlp *m, const float *feat_mean,
+                       const float *feat_std, adatm_plan *out, int *chosen, int *used_model) {
+  return guarded([&] {
+    std::vector<Candidate> all = candidate_configs(t->coo->nmodes, t->coo->dims);
+    predict_candidates(*t->coo, rank, all, t->stream.s);
+    int pick = -1;
+    if (m && feat_mean && feat_std && m->net->widths()[0] == kPlanFeatures) {
+      std::vector<float> f;
+      std::vector<double> b;
+      plan_features(*t->coo, rank, all, f, b, t->stream.s);
+      for (size_t i = 0; i < f.size(); ++i) {
+        const int k = (int)(i % kPlanFeatures);
+        f[i] = (f[i] - feat_mean[k]) / (feat_std[k] > 0 ? feat_std[k] : 1.f);
+      }
+      std::vector<float> y(all.size());
+      m->net->forward(f.data(), (int)all.size(), y.data());
+      bool finite = true;
+      for (float v : y) finite = finite && std::isfinite(v);
+      if (finite)
+        for (size_t c = 0; c < all.size(); ++c)
+          if (b[c] < 90e9 && (pick < 0 || y[c] < y[pick])) pick = (int)c;
+    }
+    if (used_model) *used_model = pick >= 0 ? 1 : 0;
+    if (pick < 0) pick = choose_candidate(all, 1, 90e9);
+    if (pick < 0) throw NoMemory("no memoization plan fits the storage limit");
+    Plan p = all[pick].plan;
+    decide_use_csfs(p);
+    plan_to_c(p, out);
+    if (chosen) *chosen = pick;
   });
 }
 

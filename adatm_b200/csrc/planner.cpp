@@ -212,6 +212,102 @@ void predict_candidates(const DevCoo &coo, uint64_t R, std::vector<Candidate> &c
   }
 }
 
+void plan_features(const DevCoo &coo, uint64_t R, const std::vector<Candidate> &cands,
+                   std::vector<float> &features, std::vector<double> &bytes, cudaStream_t s) {
+  const int N = coo.nmodes;
+  const double nnz = (double)std::max<uint64_t>(coo.nnz, 1);
+  std::map<std::vector<uint64_t>, std::vector<uint64_t>> cache;
+  auto counts_for = [&](const Group &g) {
+    std::vector<uint64_t> key(g.o_opt, g.o_opt + N);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    std::vector<uint64_t> nf(N, 0);
+    csf_count(coo, g.o_opt, nf.data(), s);
+    nf[N - 1] = coo.nnz;
+    cache[key] = nf;
+    return nf;
+  };
+  double ldmean = 0, ldmax = -1e30, ldmin = 1e30;
+  for (int m = 0; m < N; ++m) {
+    const double ld = std::log10((double)std::max<uint64_t>(coo.dims[m], 1));
+    ldmean += ld / N;
+    ldmax = std::max(ldmax, ld);
+    ldmin = std::min(ldmin, ld);
+  }
+  features.assign(cands.size() * kPlanFeatures, 0.f);
+  bytes.assign(cands.size(), 0.0);
+  for (size_t c = 0; c < cands.size(); ++c) {
+    Plan p = cands[c].plan;
+    decide_use_csfs(p);
+    std::vector<std::vector<uint64_t>> nf(p.n_csf);
+    double tree_nodes = 0, space = 0;
+    for (int g = 0; g < p.n_csf; ++g) {
+      nf[g] = counts_for(p.grp[g]);
+      for (int l = 0; l < N; ++l) tree_nodes += (double)nf[g][l];
+      space += 9.0 * nnz;  // leaf ids, FP32 + FP64 values, close depths
+      for (int l = 0; l < N - 1; ++l) space += 9.0 * (double)nf[g][l];
+      for (uint64_t d = 0; d < p.grp[g].n_imten; ++d)
+        space += 4.0 * (double)ldr_of((int)R) * (double)nf[g][p.grp[g].begin_imten - 1 - d];
+    }
+    // the walk of every mode, as the engine builds it: source level S,
+    // output level d (the mode's depth), stored levels
+    double cu = 0, su = 0, items = 0, stored = 0, fan = 0;
+    int n_leaf = 0, n_rows = 0, n_scatter = 0;
+    for (int m = 0; m < N; ++m) {
+      const int g = (int)p.use_csfs[m];
+      const Group &gp = p.grp[g];
+      int d = 0;
+      for (int l = 0; l < N; ++l)
+        if ((int)gp.o_opt[l] == m) d = l;
+      int S = N - 1;
+      if (p.use_tags[m] == 0 && gp.n_imten > 0) {
+        for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
+          stored += (double)nf[g][gp.begin_imten - 1 - deg];
+      } else if (p.use_tags[m] == 1) {
+        // mttkrp.c:1578-1588 with rcsf_reverse_mode_order (adatm_rcsf.c:313-326)
+        const uint64_t b = gp.begin_imten;
+        uint64_t rd[kMaxModes + 1] = {0};
+        uint64_t j = 0;
+        for (int64_t i = (int64_t)b; i >= 0; --i)
+          if (i != d) rd[j++] = (uint64_t)i;
+        uint64_t indeg = 0;
+        for (uint64_t i = 0; i < gp.n_imten; ++i)
+          if (b - i == rd[i]) ++indeg;
+        if (indeg > 0) S = (int)(b - indeg);
+      }
+      const double units = (double)nf[g][S];
+      if (S == N - 1) ++n_leaf;
+      else ++n_rows;
+      if (S > d) {
+        cu += units;
+        for (int l = d; l < S; ++l) items += (double)nf[g][l];
+      } else {
+        su += units;
+        ++n_scatter;
+        fan += std::log10(1.0 + units / (double)std::max<uint64_t>(coo.dims[m], 1));
+      }
+    }
+    float *x = &features[c * kPlanFeatures];
+    x[0] = (float)N;
+    x[1] = (float)std::log10(nnz);
+    x[2] = (float)std::log2((double)R);
+    x[3] = (float)ldmean;
+    x[4] = (float)ldmax;
+    x[5] = (float)ldmin;
+    x[6] = (float)p.n_grp;
+    x[7] = (float)std::log10(1.0 + cu);
+    x[8] = (float)std::log10(1.0 + su);
+    x[9] = (float)(items / nnz);
+    x[10] = (float)(stored / nnz);
+    x[11] = (float)n_leaf / N;
+    x[12] = (float)n_rows / N;
+    x[13] = (float)n_scatter / N;
+    x[14] = (float)(tree_nodes / nnz);
+    x[15] = (float)(n_scatter ? fan / n_scatter : 0.0);
+    bytes[c] = space;
+  }
+}
+
 int choose_candidate(const std::vector<Candidate> &cands, int strategy, double slimit) {
   std::vector<int> fit;
   for (size_t c = 0; c < cands.size(); ++c)

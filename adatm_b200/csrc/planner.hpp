@@ -53,6 +53,17 @@ int choose_candidate(const std::vector<Candidate> &cands, int strategy, double s
 Plan plan_analytic(const DevCoo &coo, uint64_t nfactors, int strategy,
                    std::vector<Candidate> *all, cudaStream_t s);
 
+// Features of every candidate plan for the learned plan model: tensor shape
+// (order, nnz, rank, dims) and, from the exact fiber counts of each group's
+// tree (counted on the GPU), the work of the N walks the plan runs -- units
+// of contracting and scattering walks, their upper-level items, memo rows
+// stored, scatter fan-in per output row -- and its exact storage. Row c of
+// `features` (kPlanFeatures floats) belongs to cands[c]; `bytes` receives the
+// exact device bytes of each candidate's trees plus memo rows.
+constexpr int kPlanFeatures = 16;
+void plan_features(const DevCoo &coo, uint64_t nfactors, const std::vector<Candidate> &cands,
+                   std::vector<float> &features, std::vector<double> &bytes, cudaStream_t s);
+
 // decide_use_csfs (mttkrp.c:1940-2033); fills plan.use_csfs/use_tags/n_csf.
 void decide_use_csfs(Plan &p);
 

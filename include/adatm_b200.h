@@ -253,6 +253,47 @@ int adatm_engine_fit(adatm_engine *e, double *fit);
  * rows, the tree that feeds the last mode (whose MTTKRP gives the fit's
  * inner product) still reads FP32 rows. */
 int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
+/* ------------------------------------------------------------------------ */
+/* Learned plan model (replaces the analytic cost model of                  */
+/* decide_parameters_auto, reference src/adatm_bench.c:145-272, which stays  */
+/* the fallback).                                                            */
+/* ------------------------------------------------------------------------ */
+
+#define ADATM_PLAN_FEATURES 16
+
+/* Candidate plans of decide_candidate_configs for the tensor, with
+ * ADATM_PLAN_FEATURES features per candidate (row-major into `features`,
+ * room for max_cands rows) and each candidate's exact device bytes. */
+int adatm_plan_features(const adatm_tensor *t, uint64_t rank, float *features, double *bytes,
+                        adatm_candidate *cands, int max_cands, int *ncands);
+
+/* A fully connected network: widths[0] inputs, ReLU hidden layers
+ * widths[1..nwidths-2], one linear output; He-uniform weights from seed. */
+typedef struct adatm_mlp adatm_mlp;
+int adatm_mlp_create(int nwidths, const int *widths, uint64_t seed, adatm_mlp **out);
+void adatm_mlp_free(adatm_mlp *m);
+/* Parameters, layer by layer: W (out x in, row-major) then b (out). */
+int adatm_mlp_nparams(const adatm_mlp *m, uint64_t *n);
+int adatm_mlp_set_params(adatm_mlp *m, const float *params);
+int adatm_mlp_get_params(const adatm_mlp *m, float *params);
+/* Y[rows] = net(X[rows x widths[0]]) on the GPU (host buffers). */
+int adatm_mlp_forward(adatm_mlp *m, const float *X, uint64_t rows, float *Y);
+/* Mean squared error against T and its gradient (nparams floats, the
+ * parameter layout), by the GPU backward kernels. */
+int adatm_mlp_gradient(adatm_mlp *m, const float *X, const float *T, uint64_t rows, float *grad,
+                       double *loss);
+/* Adam on seeded minibatches on the GPU; *loss = mean loss of the last epoch. */
+int adatm_mlp_train(adatm_mlp *m, const float *X, const float *T, uint64_t rows, int epochs,
+                    int batch, float lr, uint64_t seed, double *loss);
+
+/* The learned plan: every candidate's features, standardised by feat_mean /
+ * feat_std, are scored by the network (predicted log sweep time) and the
+ * lowest-scoring candidate within the reference's storage limit is chosen.
+ * With m == NULL, or a non-finite score, the analytic plan is returned and
+ * *used_model = 0. */
+int adatm_plan_learned(const adatm_tensor *t, uint64_t rank, adatm_mlp *m, const float *feat_mean,
+                       const float *feat_std, adatm_plan *out, int *chosen, int *used_model);
+
 /* G = A^T A in FP64 (R x R, row-major, device) of the device row matrix A
  * (rows x ldr floats, 16-byte aligned, first R <= 128 columns used, ldr a
  * multiple of 4): the Gram step of the CP-ALS update, with its per-block
