@@ -339,7 +339,8 @@ def _plan_to_py(p: AdatmPlan):
                         "n_imten": int(p.n_imten[g]), "o_opt": [int(p.o_opt[g][l]) for l in range(Nm)]}
                        for g in range(p.n_grp)],
             "use_csfs": [int(p.use_csfs[m]) for m in range(Nm)],
-            "use_tags": [int(p.use_tags[m]) for m in range(Nm)]}
+            "use_tags": [int(p.use_tags[m]) for m in range(Nm)],
+            "space_efficient": bool(p.space_efficient)}
 
 
 def plan_to_c(plan) -> AdatmPlan:
@@ -352,6 +353,7 @@ def plan_to_c(plan) -> AdatmPlan:
         p.n_imten[g] = gr["n_imten"]
         for l, v in enumerate(gr["o_opt"]):
             p.o_opt[g][l] = v
+    p.space_efficient = 1 if plan.get("space_efficient") else 0
     uc = plan.get("use_csfs")
     ut = plan.get("use_tags")
     if uc is None or ut is None:
@@ -704,6 +706,53 @@ class Engine:
         b = C.c_int(0)
         _check(lib().adatm_engine_launch_counts(self._h, mode, C.byref(a), C.byref(b)), "launch_counts")
         return a.value, b.value
+
+    def autotune(self, options=((128, 64), (256, 128), (512, 256), (1024, 512)), sweeps=3):
+        """Keep the fastest (chunk_leaf, chunk_rows) of `options` by timing a
+        captured sweep of each; returns its index. Initialise the factors
+        afterwards."""
+        leaf = (C.c_uint32 * len(options))(*[o[0] for o in options])
+        rows = (C.c_uint32 * len(options))(*[o[1] for o in options])
+        best = C.c_int(0)
+        _check(lib().adatm_engine_autotune(self._h, leaf, rows, len(options), sweeps, C.byref(best)),
+               "adatm_engine_autotune")
+        return best.value
+
+
+class BatchSweep:
+    """One ALS iteration of every engine in one CUDA graph; the engines must
+    stay alive while the batch is used."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (C.c_void_p * len(self.engines))(*[e._h for e in self.engines])
+        h = C.c_void_p()
+        _check(lib().adatm_batch_create(arr, len(self.engines), C.byref(h)), "adatm_batch_create")
+        self._h = h
+
+    def begin(self):
+        _check(lib().adatm_batch_begin(self._h), "adatm_batch_begin")
+
+    def time_sweeps(self, count):
+        ms = C.c_float(0)
+        _check(lib().adatm_batch_time_sweeps(self._h, count, C.byref(ms)), "adatm_batch_time_sweeps")
+        return ms.value
+
+    def kernels(self):
+        k = C.c_int(0)
+        _check(lib().adatm_batch_kernels(self._h, C.byref(k)), "adatm_batch_kernels")
+        return k.value
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().adatm_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def gram_device(A_ptr, rows, R, ldr, G_ptr):

@@ -59,7 +59,7 @@ class SpTensorT(C.Structure):
 class AdatmPlan(C.Structure):
     _fields_ = [("nmodes", C.c_int), ("n_grp", C.c_int), ("memo_mode", u64 * 8),
                 ("begin_imten", u64 * 8), ("n_imten", u64 * 8), ("o_opt", (u64 * 8) * 8),
-                ("use_csfs", u64 * 8), ("use_tags", u64 * 8)]
+                ("use_csfs", u64 * 8), ("use_tags", u64 * 8), ("space_efficient", C.c_int)]
 
 
 class AdatmCandidate(C.Structure):
@@ -148,6 +148,13 @@ _SIGS = [
     ("adatm_engine_time_mttkrp", C.c_int, [C.c_void_p, u64, C.c_int, C.POINTER(C.c_float)]),
     ("adatm_engine_fit", C.c_int, [C.c_void_p, P_f64]),
     ("adatm_engine_mttkrp_bytes", C.c_int, [C.c_void_p, u64, P_f64]),
+    ("adatm_engine_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                        C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    ("adatm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
+    ("adatm_batch_begin", C.c_int, [C.c_void_p]),
+    ("adatm_batch_time_sweeps", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
+    ("adatm_batch_kernels", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    ("adatm_batch_free", None, [C.c_void_p]),
     ("adatm_plan_features", C.c_int, [C.c_void_p, u64, C.POINTER(C.c_float), P_f64,
                                       C.POINTER(AdatmCandidate), C.c_int, C.POINTER(C.c_int)]),
     ("adatm_mlp_create", C.c_int, [C.c_int, C.POINTER(C.c_int), u64, C.POINTER(C.c_void_p)]),

@@ -171,7 +171,7 @@ std::shared_ptr<CsfHandle> make_handle(std::shared_ptr<DevCoo> coo, const Plan &
   h->plan = plan;
   for (int g = 0; g < plan.n_csf; ++g) {
     h->trees.push_back(std::make_shared<DevCsf>());
-    csf_build(*h->coo, plan.grp[g].o_opt, *h->trees.back(), h->stream.s);
+    csf_build(*h->coo, plan.tree(g).o_opt, *h->trees.back(), h->stream.s);
   }
   fill_host_trees(*h, h->coo->dims);
   std::lock_guard<std::mutex> lk(g_mu);
@@ -179,7 +179,7 @@ std::shared_ptr<CsfHandle> make_handle(std::shared_ptr<DevCoo> coo, const Plan &
   return h;
 }
 
-Plan plan_from_groups(int N, const group_properties *grp, idx_t n_grp) {
+Plan plan_from_groups(int N, const group_properties *grp, idx_t n_grp, bool space = false) {
   Plan p;
   p.nmodes = N;
   p.n_grp = (int)n_grp;
@@ -189,7 +189,8 @@ Plan plan_from_groups(int N, const group_properties *grp, idx_t n_grp) {
     p.grp[g].n_imten = grp[g].n_imten;
     for (int m = 0; m < N; ++m) p.grp[g].o_opt[m] = grp[g].o_opt[m];
   }
-  decide_use_csfs(p);
+  if (space) decide_use_csfs_space(p);
+  else decide_use_csfs(p);
   return p;
 }
 
@@ -275,6 +276,7 @@ void plan_to_c(const Plan &p, adatm_plan *o) {
     o->n_imten[g] = p.grp[g].n_imten;
     for (int l = 0; l < p.nmodes; ++l) o->o_opt[g][l] = p.grp[g].o_opt[l];
   }
+  o->space_efficient = p.space_efficient ? 1 : 0;
   for (int m = 0; m < p.nmodes; ++m) {
     o->use_csfs[m] = p.use_csfs[m];
     o->use_tags[m] = p.use_tags[m];
@@ -296,6 +298,7 @@ Plan plan_from_c(const adatm_plan *c) {
     p.use_tags[m] = c->use_tags[m];
   }
   p.n_csf = p.n_grp;
+  if (c->space_efficient) decide_use_csfs_space(p);
   return p;
 }
 
@@ -313,6 +316,11 @@ std::shared_ptr<DevCoo> coo_of(sptensor_t *tt, cudaStream_t s) {
 struct adatm_tensor {
   StreamOwner stream;
   std::shared_ptr<DevCoo> coo;
+};
+
+struct adatm_batch {
+  StreamOwner stream;
+  std::unique_ptr<BatchSweep> batch;
 };
 
 struct adatm_mlp {
@@ -593,7 +601,9 @@ splatt_csf *csf_alloc_adaptive(sptensor_t *const tt, group_properties *const grp
     (void)opts;
     StreamOwner s;
     auto coo = coo_of(tt, s.s);
-    Plan p = plan_from_groups((int)tt->nmodes, grp_prop, n_grp);
+    const bool space =
+        opts != nullptr && (int)opts[SPLATT_OPTION_CSF_ALLOC] == SPLATT_ADAPTIVE_SPACE_EFFICIENT;
+    Plan p = plan_from_groups((int)tt->nmodes, grp_prop, n_grp, space);
     check_plan(p);
     auto h = make_handle(coo, p);
     *n_csf = (idx_t)h->n_csf;
@@ -613,15 +623,19 @@ rcsf_seq_adaptive *rcsf_alloc_adaptive(splatt_csf *const ct, idx_t const nfactor
   int rc = guarded([&] {
     auto h = find_csf(ct);
     h->engine(nfactors);  // memo rows in HBM
-    ret = (rcsf_seq_adaptive *)calloc(n_grp ? n_grp : 1, sizeof(rcsf_seq_adaptive));
+    (void)grp_prop;
+    (void)n_grp;
+    const Plan &plan = h->plan;
+    ret = (rcsf_seq_adaptive *)calloc(plan.n_csf ? plan.n_csf : 1, sizeof(rcsf_seq_adaptive));
     idx_t j = 0;
-    for (idx_t g = 0; g < n_grp; ++g) {
-      if (grp_prop[g].n_imten == 0) continue;
+    for (int t = 0; t < plan.n_csf; ++t) {  // one memo sequence per memoizing tree
+      const Group &gp = plan.tree(t);
+      if (gp.n_imten == 0) continue;
       rcsf_seq_adaptive &sq = ret[j++];
-      sq.begin_imten = grp_prop[g].begin_imten;
-      sq.n_imten = grp_prop[g].n_imten;
+      sq.begin_imten = gp.begin_imten;
+      sq.n_imten = gp.n_imten;
       sq.rcsfs = (splatt_csf *)calloc(sq.n_imten, sizeof(splatt_csf));
-      const splatt_csf &c = ct[g];
+      const splatt_csf &c = ct[t];
       // memo tree layout of p_rcsf_alloc_untiled_adaptive (adatm_rcsf.c:216-278)
       for (idx_t deg = 0; deg < sq.n_imten; ++deg) {
         splatt_csf &o = sq.rcsfs[deg];
@@ -682,8 +696,9 @@ size_t rcsf_storage_adaptive(rcsf_seq_adaptive const *const seq_rcsf, idx_t cons
 
 void decide_use_csfs(idx_t const nmodes, group_properties *const grp_prop, int const n_grp,
                      idx_t const n_csf, idx_t *use_csfs, idx_t *use_tags) {
-  (void)n_csf;
-  Plan p = plan_from_groups((int)nmodes, grp_prop, (idx_t)n_grp);
+  // the reference takes the SPACE_EFFICIENT branch when fewer trees than
+  // groups were built (mttkrp.c:1976)
+  Plan p = plan_from_groups((int)nmodes, grp_prop, (idx_t)n_grp, n_csf != (idx_t)n_grp);
   for (idx_t m = 0; m < nmodes; ++m) {
     use_csfs[m] = p.use_csfs[m];
     use_tags[m] = p.use_tags[m];
@@ -842,11 +857,11 @@ int adatm_rcsf_pull(rcsf_seq_adaptive *rs_seq, idx_t n_rcsf) {
       const splatt_csf &r0 = rs_seq[j].rcsfs[0];
       const uint64_t R = r0.dims[r0.nmodes - 1];
       Engine &e = h->engine(R);
-      int g = -1;
-      for (int gg = 0, k = 0; gg < e.plan().n_grp; ++gg) {
-        if (e.plan().grp[gg].n_imten == 0) continue;
+      int g = -1;  // the j-th memoizing tree
+      for (int tt = 0, k = 0; tt < e.plan().n_csf; ++tt) {
+        if (e.plan().tree(tt).n_imten == 0) continue;
         if ((idx_t)k == j) {
-          g = gg;
+          g = tt;
           break;
         }
         ++k;
@@ -1146,6 +1161,46 @@ int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes) {
   });
 }
 
+int adatm_engine_autotune(adatm_engine *e, const uint32_t *chunk_leaf, const uint32_t *chunk_rows,
+                          int n, int sweeps, int *best) {
+  return guarded([&] {
+    if (n < 1 || !chunk_leaf || !chunk_rows) throw BadInput("adatm_engine_autotune: no options");
+    std::vector<std::pair<uint32_t, uint32_t>> opts;
+    for (int i = 0; i < n; ++i) opts.emplace_back(chunk_leaf[i], chunk_rows[i]);
+    const int b = e->eng->autotune(opts, sweeps);
+    e->graph = false;
+    if (best) *best = b;
+  });
+}
+
+int adatm_batch_create(adatm_engine *const *engines, int n, adatm_batch **out) {
+  return guarded([&] {
+    if (n < 1 || !engines || !out) throw BadInput("adatm_batch_create: no engines");
+    std::vector<Engine *> es;
+    for (int i = 0; i < n; ++i) {
+      if (!engines[i]) throw BadInput("adatm_batch_create: null engine");
+      es.push_back(engines[i]->eng.get());
+    }
+    auto b = std::make_unique<adatm_batch>();
+    b->batch = std::make_unique<BatchSweep>(es, b->stream.s);
+    *out = b.release();
+  });
+}
+
+int adatm_batch_begin(adatm_batch *b) {
+  return guarded([&] { b->batch->begin(); });
+}
+
+int adatm_batch_time_sweeps(adatm_batch *b, int count, float *ms) {
+  return guarded([&] { *ms = b->batch->time_sweeps(count); });
+}
+
+int adatm_batch_kernels(const adatm_batch *b, int *per_sweep) {
+  return guarded([&] { *per_sweep = b->batch->kernels_per_sweep(); });
+}
+
+void adatm_batch_free(adatm_batch *b) { delete b; }
+
 int adatm_plan_features(const adatm_tensor *t, uint64_t rank, float *features, double *bytes,
                         adatm_candidate *cands, int max_cands, int *ncands) {
   return guarded([&] {
@@ -1285,11 +1340,12 @@ int adatm_engine_launch_counts(adatm_engine *e, uint64_t mode, int *per_sweep, i
 
 namespace {
 int adatm_engine_memo_raw(Engine *g, int grp, int deg, double *out) {
+  // grp: tree index (the group index in TIME_EFFICIENT plans)
   return guarded([&] {
     const Plan &p = g->plan();
-    if (grp < 0 || grp >= p.n_grp || deg < 0 || (uint64_t)deg >= p.grp[grp].n_imten)
+    if (grp < 0 || grp >= p.n_csf || deg < 0 || (uint64_t)deg >= p.tree(grp).n_imten)
       throw BadInput("memo tree out of range");
-    const uint64_t lvl = p.grp[grp].begin_imten - 1 - deg;
+    const uint64_t lvl = p.tree(grp).begin_imten - 1 - deg;
     const uint64_t rows = g->csf(grp).nfibs[lvl];
     pull_rows(*g, g->memo_rows(grp, deg), rows, out);
   });

@@ -23,12 +23,12 @@ Engine::Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<De
   if (csf_.empty()) {
     for (int g = 0; g < plan_.n_csf; ++g) {
       csf_.emplace_back(std::make_shared<DevCsf>());
-      csf_build(*coo_, plan_.grp[g].o_opt, *csf_.back(), stream_);
+      csf_build(*coo_, plan_.tree(g).o_opt, *csf_.back(), stream_);
     }
   }
   if ((int)csf_.size() != plan_.n_csf) throw BadInput("tree count does not match the plan");
   for (int g = 0; g < plan_.n_csf; ++g) {
-    const Group &gp = plan_.grp[g];
+    const Group &gp = plan_.tree(g);
     for (uint64_t deg = 0; deg < gp.n_imten; ++deg) {
       const uint64_t lvl = gp.begin_imten - 1 - deg;
       const size_t n = (size_t)csf_[g]->nfibs[lvl] * ldr_;
@@ -60,9 +60,126 @@ Engine::Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<De
 }
 
 Engine::~Engine() {
+  drop_graph();
+  if (staging_) cudaFreeHost(staging_);
+}
+
+void Engine::drop_graph() {
   if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
   if (graph_) cudaGraphDestroy(graph_);
-  if (staging_) cudaFreeHost(staging_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
+}
+
+void Engine::set_chunks(uint32_t chunk_leaf, uint32_t chunk_rows) {
+  if (chunk_leaf == 0 || chunk_rows == 0) throw BadInput("chunk sizes must be positive");
+  drop_graph();
+  opt_.chunk_leaf = chunk_leaf;
+  opt_.chunk_rows = chunk_rows;
+  build_walks();
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+float Engine::time_sweeps(int count) {
+  cudaEvent_t a, b;
+  ADATM_CUDA(cudaEventCreate(&a));
+  ADATM_CUDA(cudaEventCreate(&b));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  ADATM_CUDA(cudaEventRecord(a, stream_));
+  for (int i = 0; i < count; ++i) sweep();
+  ADATM_CUDA(cudaEventRecord(b, stream_));
+  ADATM_CUDA(cudaEventSynchronize(b));
+  float ms = 0;
+  ADATM_CUDA(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms;
+}
+
+int Engine::autotune(const std::vector<std::pair<uint32_t, uint32_t>> &options, int sweeps) {
+  if (options.empty()) throw BadInput("no chunk options to tune");
+  int best = -1;
+  float best_ms = 0;
+  for (size_t i = 0; i < options.size(); ++i) {
+    set_chunks(options[i].first, options[i].second);
+    als_begin();
+    capture_graph();
+    time_sweeps(1);
+    const float ms = time_sweeps(std::max(1, sweeps));
+    if (best < 0 || ms < best_ms) {
+      best = (int)i;
+      best_ms = ms;
+    }
+  }
+  set_chunks(options[best].first, options[best].second);
+  return best;
+}
+
+BatchSweep::BatchSweep(std::vector<Engine *> engines, cudaStream_t stream)
+    : e_(std::move(engines)), s_(stream) {
+  if (e_.empty()) throw BadInput("an empty batch");
+  for (Engine *e : e_)
+    if (!e) throw BadInput("a null engine in the batch");
+  ADATM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+  join_.resize(e_.size(), nullptr);
+  for (auto &ev : join_) ADATM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+}
+
+BatchSweep::~BatchSweep() {
+  if (exec_) cudaGraphExecDestroy(exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  for (auto ev : join_)
+    if (ev) cudaEventDestroy(ev);
+  if (fork_) cudaEventDestroy(fork_);
+}
+
+void BatchSweep::begin() {
+  for (Engine *e : e_) e->als_begin();
+  if (exec_) return;
+  ADATM_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+  try {
+    ADATM_CUDA(cudaEventRecord(fork_, s_));
+    for (size_t i = 0; i < e_.size(); ++i) {
+      ADATM_CUDA(cudaStreamWaitEvent(e_[i]->stream(), fork_, 0));
+      e_[i]->sweep_eager();
+      ADATM_CUDA(cudaEventRecord(join_[i], e_[i]->stream()));
+      ADATM_CUDA(cudaStreamWaitEvent(s_, join_[i], 0));
+    }
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(s_, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  ADATM_CUDA(cudaStreamEndCapture(s_, &graph_));
+  ADATM_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+}
+
+void BatchSweep::sweep() {
+  if (!exec_) throw BadInput("the batch has not begun");
+  ADATM_CUDA(cudaGraphLaunch(exec_, s_));
+}
+
+float BatchSweep::time_sweeps(int count) {
+  cudaEvent_t a, b;
+  ADATM_CUDA(cudaEventCreate(&a));
+  ADATM_CUDA(cudaEventCreate(&b));
+  ADATM_CUDA(cudaStreamSynchronize(s_));
+  ADATM_CUDA(cudaEventRecord(a, s_));
+  for (int i = 0; i < count; ++i) sweep();
+  ADATM_CUDA(cudaEventRecord(b, s_));
+  ADATM_CUDA(cudaEventSynchronize(b));
+  float ms = 0;
+  ADATM_CUDA(cudaEventElapsedTime(&ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms;
+}
+
+int BatchSweep::kernels_per_sweep() const {
+  int k = 0;
+  for (Engine *e : e_) k += e->kernels_per_sweep();
+  return k;
 }
 
 float *Engine::staging(size_t n) {
@@ -95,7 +212,7 @@ void Engine::build_walks() {
     const int g = (int)plan_.use_csfs[m];
     const int tag = (int)plan_.use_tags[m];
     const DevCsf &c = *csf_[g];
-    const Group &gp = plan_.grp[g];
+    const Group &gp = plan_.tree(g);
     const int d = depth_of(c, m);
     auto direct = std::make_unique<TreeWalk>();
     direct->csf = &c;

@@ -77,6 +77,18 @@ class Engine {
   // compulsory HBM bytes of the MTTKRP of `mode` (roofline numerator)
   double mttkrp_bytes(int mode) const;
 
+  // Rebuild the walk schedules with other chunk sizes (drops a captured
+  // graph). Factors, Grams and memo rows stay as they are.
+  void set_chunks(uint32_t chunk_leaf, uint32_t chunk_rows);
+  uint32_t chunk_leaf() const { return opt_.chunk_leaf; }
+  uint32_t chunk_rows() const { return opt_.chunk_rows; }
+  // Time `count` graph-replayed sweeps (CUDA events, ms total).
+  float time_sweeps(int count);
+  // Chunk autotuner: time a captured sweep with every (leaf, rows) pair and
+  // keep the fastest; returns its index. Runs sweeps, so it changes the
+  // factors: initialise them afterwards.
+  int autotune(const std::vector<std::pair<uint32_t, uint32_t>> &options, int sweeps);
+
  private:
   void build_walks();
   LevelFactors level_factors(int g, FactorType ft) const;
@@ -101,6 +113,32 @@ class Engine {
   float *staging(size_t n);
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
+  void drop_graph();
+};
+
+// Many independent tensors swept together: one CUDA graph holds one ALS
+// iteration of every engine, each engine's kernels on a branch of its own
+// (its stream, forked from and joined to the batch's stream), so the small
+// launches of uneven tensors overlap on the GPU and the host launches one
+// graph per iteration. The engines must outlive the batch.
+class BatchSweep {
+ public:
+  BatchSweep(std::vector<Engine *> engines, cudaStream_t stream);
+  ~BatchSweep();
+  BatchSweep(const BatchSweep &) = delete;
+  BatchSweep &operator=(const BatchSweep &) = delete;
+  void begin();                 // als_begin of every engine, then capture
+  void sweep();                 // one graph launch
+  float time_sweeps(int count); // CUDA events on the batch stream, ms total
+  int kernels_per_sweep() const;
+
+ private:
+  std::vector<Engine *> e_;
+  cudaStream_t s_;
+  cudaEvent_t fork_ = nullptr;
+  std::vector<cudaEvent_t> join_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
 };
 
 }  // namespace adatm

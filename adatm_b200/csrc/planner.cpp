@@ -242,12 +242,12 @@ void plan_features(const DevCoo &coo, uint64_t R, const std::vector<Candidate> &
     std::vector<std::vector<uint64_t>> nf(p.n_csf);
     double tree_nodes = 0, space = 0;
     for (int g = 0; g < p.n_csf; ++g) {
-      nf[g] = counts_for(p.grp[g]);
+      nf[g] = counts_for(p.tree(g));
       for (int l = 0; l < N; ++l) tree_nodes += (double)nf[g][l];
       space += 9.0 * nnz;  // leaf ids, FP32 + FP64 values, close depths
       for (int l = 0; l < N - 1; ++l) space += 9.0 * (double)nf[g][l];
-      for (uint64_t d = 0; d < p.grp[g].n_imten; ++d)
-        space += 4.0 * (double)ldr_of((int)R) * (double)nf[g][p.grp[g].begin_imten - 1 - d];
+      for (uint64_t d = 0; d < p.tree(g).n_imten; ++d)
+        space += 4.0 * (double)ldr_of((int)R) * (double)nf[g][p.tree(g).begin_imten - 1 - d];
     }
     // the walk of every mode, as the engine builds it: source level S,
     // output level d (the mode's depth), stored levels
@@ -255,7 +255,7 @@ void plan_features(const DevCoo &coo, uint64_t R, const std::vector<Candidate> &
     int n_leaf = 0, n_rows = 0, n_scatter = 0;
     for (int m = 0; m < N; ++m) {
       const int g = (int)p.use_csfs[m];
-      const Group &gp = p.grp[g];
+      const Group &gp = p.tree(g);
       int d = 0;
       for (int l = 0; l < N; ++l)
         if ((int)gp.o_opt[l] == m) d = l;
@@ -335,10 +335,77 @@ Plan plan_analytic(const DevCoo &coo, uint64_t R, int strategy, std::vector<Cand
   return p;
 }
 
+namespace {
+// locate_ind_special (adatm_utils.c:9-29): position of ele among the memo
+// modes, x.5 between two of them, -1 if none. The reference's loop stops
+// after its first pass (the `break` at :23), so only positions 0 and 1 and
+// the tail are ever found; that behaviour is kept, it decides the plan.
+double locate_ind_special(const uint64_t *array, uint64_t length, uint64_t ele, uint64_t nmodes) {
+  double loc = -1;
+  if (array[0] == ele) loc = 0;
+  for (uint64_t i = 1; i < length; ++i) {
+    if (array[i] == ele) loc = (double)i;
+    else if (array[i - 1] < ele && ele < array[i]) loc = (double)i - 0.5;
+    break;
+  }
+  if (array[length - 1] < ele && ele < nmodes) loc = (double)length - 0.5;
+  return loc;
+}
+}  // namespace
+
+void decide_use_csfs_space(Plan &p) {
+  const int N = p.nmodes;
+  int memo_groups[kMaxModes];
+  uint64_t csf_modes[kMaxModes];
+  int n = 0;
+  for (int g = 0; g < p.n_grp; ++g)
+    if (p.grp[g].n_imten > 0) {
+      memo_groups[n] = g;
+      csf_modes[n] = p.grp[g].memo_mode;
+      ++n;
+    }
+  if (p.n_grp == 1 || n == 0 || n == p.n_grp) {
+    decide_use_csfs(p);
+    return;
+  }
+  p.space_efficient = true;
+  p.n_csf = n;
+  for (int t = 0; t < kMaxModes; ++t) p.tree_group[t] = t < n ? memo_groups[t] : 0;
+  // mttkrp.c:1976-2029. Modes the reference leaves unassigned (its
+  // locate_ind_special misses them) recompute on tree 0.
+  bool set[kMaxModes] = {false};
+  auto assign = [&](uint64_t first, uint64_t stop, double loc) {
+    if (loc < 0) return;
+    const uint64_t t = (uint64_t)loc;
+    const bool exact = loc - (double)t == 0;
+    p.use_csfs[first] = t;
+    p.use_tags[first] = exact ? 0 : 2;
+    set[first] = true;
+    for (uint64_t rm = first + 1; rm < stop; ++rm) {
+      p.use_csfs[rm] = t;
+      p.use_tags[rm] = exact ? 1 : 2;
+      set[rm] = true;
+    }
+  };
+  for (int g = 0; g + 1 < p.n_grp; ++g) {
+    const uint64_t mode = p.grp[g].memo_mode;
+    assign(mode, p.grp[g + 1].memo_mode, locate_ind_special(csf_modes, n, mode, N));
+    const uint64_t last = p.grp[p.n_grp - 1].memo_mode;
+    assign(last, (uint64_t)N, locate_ind_special(csf_modes, n, last, N));
+  }
+  for (int m = 0; m < N; ++m)
+    if (!set[m]) {
+      p.use_csfs[m] = 0;
+      p.use_tags[m] = 2;
+    }
+}
+
 void decide_use_csfs(Plan &p) {
   // TIME_EFFICIENT: one tree per group (mttkrp.c:1956-1975)
   const int N = p.nmodes;
   p.n_csf = p.n_grp;
+  p.space_efficient = false;
+  for (int t = 0; t < kMaxModes; ++t) p.tree_group[t] = t;
   for (int g = 0; g < p.n_grp; ++g) {
     const uint64_t mode = p.grp[g].memo_mode;
     const uint64_t stop = (g + 1 < p.n_grp) ? p.grp[g + 1].memo_mode : (uint64_t)N;

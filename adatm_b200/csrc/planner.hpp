@@ -28,6 +28,11 @@ struct Plan {
   uint64_t use_csfs[kMaxModes] = {0};
   uint64_t use_tags[kMaxModes] = {0};
   int n_csf = 0;
+  // tree t is built in the order of group tree_group[t] (identity except in
+  // SPACE_EFFICIENT plans, whose trees are the memoizing groups only)
+  int tree_group[kMaxModes] = {0, 1, 2, 3, 4, 5, 6, 7};
+  bool space_efficient = false;
+  const Group &tree(int t) const { return grp[tree_group[t]]; }
 };
 
 struct Candidate {
@@ -66,6 +71,11 @@ void plan_features(const DevCoo &coo, uint64_t nfactors, const std::vector<Candi
 
 // decide_use_csfs (mttkrp.c:1940-2033); fills plan.use_csfs/use_tags/n_csf.
 void decide_use_csfs(Plan &p);
+// SPACE_EFFICIENT plans (adatm_rcsf.c:528-552, mttkrp.c:1976-2029): trees
+// only for the groups that memoize; every other group's modes recompute
+// (tag 2) on the tree locate_ind_special names. A plan with one group, or
+// with no memoizing group, stays TIME_EFFICIENT.
+void decide_use_csfs_space(Plan &p);
 
 // SPLATT's plain allocations as plans: ONEMODE (one tree, modes by dimension
 // ascending), TWOMODE (that tree plus one rooted at the largest mode),

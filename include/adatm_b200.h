@@ -169,6 +169,7 @@ typedef struct adatm_plan {
   uint64_t o_opt[8][8];
   uint64_t use_csfs[8];
   uint64_t use_tags[8];
+  int space_efficient; /* trees only for memoizing groups (SPLATT_ADAPTIVE_SPACE_EFFICIENT) */
 } adatm_plan;
 
 typedef struct adatm_candidate {
@@ -253,6 +254,26 @@ int adatm_engine_fit(adatm_engine *e, double *fit);
  * rows, the tree that feeds the last mode (whose MTTKRP gives the fit's
  * inner product) still reads FP32 rows. */
 int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
+/* ------------------------------------------------------------------------ */
+/* Batched sweeps of many tensors and the chunk autotuner                   */
+/* ------------------------------------------------------------------------ */
+
+/* Time a captured sweep with each (chunk_leaf[i], chunk_rows[i]) and keep the
+ * fastest (*best = its index). Runs sweeps: initialise the factors after. */
+int adatm_engine_autotune(adatm_engine *e, const uint32_t *chunk_leaf, const uint32_t *chunk_rows,
+                          int n, int sweeps, int *best);
+
+/* One ALS iteration of every engine in one CUDA graph (each engine on its
+ * own branch). The engines must outlive the batch. */
+typedef struct adatm_batch adatm_batch;
+int adatm_batch_create(adatm_engine *const *engines, int n, adatm_batch **out);
+/* Grams and norms of every engine, then the graph capture. */
+int adatm_batch_begin(adatm_batch *b);
+/* `count` graph launches timed with CUDA events (*ms total). */
+int adatm_batch_time_sweeps(adatm_batch *b, int count, float *ms);
+int adatm_batch_kernels(const adatm_batch *b, int *per_sweep);
+void adatm_batch_free(adatm_batch *b);
+
 /* ------------------------------------------------------------------------ */
 /* Learned plan model (replaces the analytic cost model of                  */
 /* decide_parameters_auto, reference src/adatm_bench.c:145-272, which stays  */

@@ -1,0 +1,56 @@
+"""Batched sweeps of several uneven tensors in one CUDA graph, and the chunk
+autotuner: both leave the numbers of a sweep unchanged."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [([300, 200, 100], 20000, None), ([120, 90, 80, 70], 30000, 1.2),
+          ([60, 50, 40, 30, 20], 25000, 1.1), ([500, 40, 300], 15000, 1.4),
+          ([90, 80, 70, 60], 5000, None), ([2000, 1500, 900], 60000, 1.3)]
+
+
+def engines(A, R=16):
+    out = []
+    for k, (dims, nnz, alpha) in enumerate(SHAPES):
+        t = A.Tensor.generate(dims, nnz, alpha=alpha, seed=100 + k)
+        plan, _, _ = A.plan_analytic(t, R)
+        out.append((t, A.Engine(t, R, plan)))
+    return out
+
+
+def test_batched_graph_matches_each_engine(gpu):
+    A = gpu
+    ref = []
+    for t, e in engines(A):
+        e.init_factors(0)
+        ref.append(e.als(4, 0.0, graph=True)["trace"])
+    pairs = engines(A)
+    es = [e for _, e in pairs]
+    for e in es:
+        e.init_factors(0)
+    b = A.BatchSweep(es)
+    b.begin()
+    b.time_sweeps(4)
+    for e, r in zip(es, ref):
+        assert abs(e.fit() - r[-1]) < 1e-5
+    assert b.kernels() == sum(e.launch_counts(0)[0] for e in es)
+    b.free()
+
+
+def test_autotune_keeps_results(gpu):
+    A = gpu
+    t = A.Tensor.generate([400, 300, 200, 100], 80000, alpha=1.2, seed=7)
+    plan, _, _ = A.plan_analytic(t, 16)
+    e0 = A.Engine(t, 16, plan)
+    e0.init_factors(0)
+    r0 = e0.als(3, 0.0)
+    e1 = A.Engine(t, 16, plan)
+    best = e1.autotune(((32, 16), (256, 128), (1024, 512)), sweeps=2)
+    assert best in (0, 1, 2)
+    e1.init_factors(0)
+    r1 = e1.als(3, 0.0)
+    assert abs(r0["fit"] - r1["fit"]) < 1e-5
+    m0 = e0.mttkrp(1)
+    m1 = e1.mttkrp(1)
+    assert np.max(np.abs(m0 - m1)) <= 1e-4 * np.max(np.abs(m0))
