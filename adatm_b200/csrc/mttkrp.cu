@@ -332,18 +332,23 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
         if (!FULL && k0 >= cnt) break;
         fv<V> g[SB];
         fv<V> m[LEAF ? 1 : SB];
+        float vv[LEAF ? SB : 1];
 #pragma unroll
         for (int q = 0; q < SB; ++q) {
           const int k = k0 + q;
-          const bool ok = act && (FULL || k < cnt);
-          g[q] = Us.load(ustage[k].x, ok);
-          if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok);
+          // lanes past the rank read column 0 through Us's base, so only
+          // the units past the batch need the row-0 substitute
+          const bool ok = FULL || k < cnt;
+          const uint2 e = ustage[k];
+          g[q] = Us.load(e.x, ok);
+          if constexpr (LEAF) vv[q] = __uint_as_float(e.y);
+          if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok && act);
         }
 #pragma unroll
         for (int q = 0; q < SB; ++q) {
           const int k = k0 + q;
           if (FULL || k < cnt) {
-            if constexpr (LEAF) fv_axpy(acc, __uint_as_float(ustage[k].y), g[q]);
+            if constexpr (LEAF) fv_axpy(acc, vv[LEAF ? q : 0], g[q]);
             else fv_fma(acc, m[LEAF ? 0 : q], g[q]);
             if ((M >> k) & 1u) {
               items[j * 32 + lane] = acc;

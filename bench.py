@@ -270,8 +270,13 @@ def run_ours(args):
     nmodes, nnz, dims = t.info()
     gen_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    plan, cands, chosen = A.plan_analytic(t, RANK)
+    # the chosen plan: the learned plan model shipped with the package (the
+    # analytic model when it is absent); the analytic plan is timed beside it
+    model_path = os.path.join(HERE, "adatm_b200", "planner_data", "plan_model.npz")
+    model = A.PlanModel.load(model_path) if os.path.exists(model_path) else None
+    plan, chosen_idx, model_used = A.plan_learned(t, RANK, model)
     plan_s = time.perf_counter() - t0
+    analytic_plan, _, analytic_idx = A.plan_analytic(t, RANK)
     t0 = time.perf_counter()
     eng = A.Engine(t, RANK, plan)
     build_s = time.perf_counter() - t0
@@ -323,6 +328,15 @@ def run_ours(args):
     plain.time_sweeps(W)
     plain_ms = plain.time_sweeps(K) / K
     plain.free()
+    if analytic_idx != chosen_idx:
+        an = A.Engine(t, RANK, analytic_plan)
+        an.init_factors(SEED)
+        an.als_begin(graph=True)
+        an.time_sweeps(W)
+        analytic_ms = an.time_sweeps(K) / K
+        an.free()
+    else:
+        analytic_ms = None  # same plan as the chosen one
     bf = A.Engine(t, RANK, plan, bf16=True)
     bf.init_factors(SEED)
     bf.als_begin(graph=True)
@@ -392,7 +406,10 @@ def run_ours(args):
                 "call": "cpd_als_iterate_adaptive(NITER=1) with host FP64 factors per step"},
         "chosen_vs_plain": {"memo_fp32_sweep_ms": ms_step, "memo_bf16_sweep_ms": bf_ms,
                             "plain_rcsf_fp32_sweep_ms": plain_ms,
-                            "speedup_memo_vs_plain": plain_ms / ms_step},
+                            "speedup_memo_vs_plain": plain_ms / ms_step,
+                            "plan_model": "learned" if model_used else "analytic",
+                            "chosen_candidate": chosen_idx, "analytic_candidate": analytic_idx,
+                            "analytic_plan_sweep_ms": analytic_ms if analytic_ms is not None else ms_step},
         "mttkrp": {"ms_per_mode": mode_ms, "sequence_gbs": seq_gbs,
                    "bytes_per_mode": [eng.mttkrp_bytes(m) for m in range(nmodes)]},
         "fit_after_steps": fit,

@@ -69,3 +69,21 @@ def test_plan_features_and_learned_plan(gpu):
     e0.init_factors(0)
     r0 = e0.als(3, 0.0)
     assert abs(r1["fit"] - r0["fit"]) < 1e-4
+
+
+def test_committed_model_through_the_library(gpu):
+    """The shipped model loaded into the GPU network picks, through
+    adatm_plan_learned, the candidate its numpy forward ranks first."""
+    import os
+    from conftest import ROOT
+    from _mlp_ref import forward
+    A = gpu
+    path = os.path.join(ROOT, "adatm_b200", "planner_data", "plan_model.npz")
+    model = A.PlanModel.load(path)
+    t = A.Tensor.generate([3000, 1200, 800, 400, 200, 60], 600_000, alpha=1.25, seed=11)
+    X, _, _ = A.plan_features(t, 32)
+    z = np.load(path)
+    pred, _, _ = forward(z["params"], [int(w) for w in z["widths"]], (X - z["mean"]) / z["std"])
+    np.testing.assert_allclose(model.predict(X), pred, rtol=1e-4, atol=1e-4)
+    plan, chosen, used = A.plan_learned(t, 32, model)
+    assert used and chosen == int(np.argmin(pred))
