@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
   if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
   const RowSrc<V, FT> Us(a.U_src, a.ldr, col, act);
   fv<V> acc = fv_fill<V>(0.f);  // open node of level S-1
-  constexpr int SB = 8 / V;     // unit rows in flight per lane
+  constexpr int SB = 16 / V;    // unit rows in flight per lane
   const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
   const uint64_t u1 = min(u0 + a.chunk, a.nunits);
   for (uint64_t base = u0; base < u1; base += kBatch) {
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
         const RowSrc<V, FT> Ul(a.U[l], a.ldr, col, act);
         fv<V> cl = carry[(l - 1) * 32 + lane];
         int jj = 0;
-#pragma unroll 4
+#pragma unroll 8
         for (int i = 0; i < n; ++i) {
           const fv<V> row = Ul.load(__shfl_sync(~0u, fid, i), true);
           fv_fma(cl, items[i * 32 + lane], row);
