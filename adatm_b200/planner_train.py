@@ -4,15 +4,17 @@
     python -m adatm_b200.planner_train train --data DATA.npz --model MODEL.npz
     python -m adatm_b200.planner_train eval  --model MODEL.npz [--big]
 
-`make` draws seeded synthetic tensors (order 4..8, dims log-uniform in
-[50, 100000], nnz log-uniform in [1e5, --max-nnz], Zipf alpha uniform in
-[1.0, 1.6], values U(0, 1), R = 32), enumerates the candidate plans of
+`make` draws seeded synthetic tensors (order --min-order..8, dims
+log-uniform in [50, 100000], nnz log-uniform in [--min-nnz, --max-nnz], Zipf
+alpha uniform in [1.0, 1.6], values U(0, 1), R drawn from --ranks),
+enumerates the candidate plans of
 decide_candidate_configs, and times a CP-ALS sweep of every candidate with the
 library's own kernels (CUDA-graph replays, CUDA events): the label of a
 (tensor, candidate) row is log10(ms per sweep). The analytic model's choice is
 kept beside it.
 
-`train` standardises the features, holds out the last 20% of tensors, trains
+`train` (one or more --data sets) standardises the features, holds out the
+last 20% of every set's tensors, trains
 the network on the GPU (the library's forward, backward and Adam kernels) to
 regress the label, and reports the regret of the learned and the analytic
 choice on the held-out tensors: regret = time(chosen) / time(best) - 1, the
@@ -40,17 +42,18 @@ WIDTHS = [A.PLAN_FEATURES, 64, 64, 1]
 RANK = 32
 
 
-def draw_tensor_spec(seed, max_nnz):
+def draw_tensor_spec(seed, max_nnz, min_nnz=1e5, min_order=4, ranks=(RANK,)):
     rng = np.random.default_rng(seed)
-    N = int(rng.integers(4, 9))
+    N = int(rng.integers(min_order, 9))
     dims = [int(round(math.exp(rng.uniform(math.log(50), math.log(100000))))) for _ in range(N)]
-    nnz = int(round(math.exp(rng.uniform(math.log(1e5), math.log(max_nnz)))))
+    nnz = int(round(math.exp(rng.uniform(math.log(min_nnz), math.log(max_nnz)))))
     alpha = float(rng.uniform(1.0, 1.6))
-    return N, dims, nnz, alpha
+    R = int(ranks[int(rng.integers(0, len(ranks)))]) if len(ranks) > 1 else int(ranks[0])
+    return N, dims, nnz, alpha, R
 
 
-def time_plan(t, plan, sweeps=5):
-    e = A.Engine(t, RANK, plan)
+def time_plan(t, plan, sweeps=5, R=RANK):
+    e = A.Engine(t, R, plan)
     try:
         e.init_factors(0)
         e.als_begin(graph=True)
@@ -60,28 +63,30 @@ def time_plan(t, plan, sweeps=5):
         e.free()
 
 
-def measure_tensor(t, sweeps=5):
+def measure_tensor(t, sweeps=5, R=RANK):
     """Features, exact bytes, candidates, per-candidate ms and the analytic
     choice for one tensor."""
-    X, nbytes, cands = A.plan_features(t, RANK)
-    _, _, chosen = A.plan_analytic(t, RANK)
+    X, nbytes, cands = A.plan_features(t, R)
+    _, _, chosen = A.plan_analytic(t, R)
     ms = np.full(len(cands), np.nan)
     for c, cand in enumerate(cands):
         if nbytes[c] >= 90e9:
             continue
         plan = {"nmodes": cand["nmodes"], "groups": cand["groups"]}
-        ms[c] = time_plan(t, plan, sweeps)
+        ms[c] = time_plan(t, plan, sweeps, R)
     return X, nbytes, cands, ms, chosen
 
 
 def make(args):
     A.lib().adatm_set_device(0)
     rows, labels, tid, cidx, analytic, specs = [], [], [], [], [], []
+    ranks = [int(r) for r in args.ranks.split(",")]
     for k in range(args.tensors):
         seed = args.seed0 + k
-        N, dims, nnz, alpha = draw_tensor_spec(seed, args.max_nnz)
+        N, dims, nnz, alpha, R = draw_tensor_spec(seed, args.max_nnz, args.min_nnz, args.min_order,
+                                                  ranks)
         t = A.Tensor.generate(dims, nnz, alpha=alpha, seed=seed)
-        X, nbytes, cands, ms, chosen = measure_tensor(t, args.sweeps)
+        X, nbytes, cands, ms, chosen = measure_tensor(t, args.sweeps, R)
         t.free()
         for c in range(len(cands)):
             if np.isfinite(ms[c]):
@@ -90,8 +95,9 @@ def make(args):
                 tid.append(k)
                 cidx.append(c)
         analytic.append(chosen)
-        specs.append(json.dumps({"seed": seed, "N": N, "dims": dims, "nnz": nnz, "alpha": alpha}))
-        print(f"tensor {k} N={N} nnz={nnz} cands={len(cands)} ms={np.round(ms, 3).tolist()} "
+        specs.append(json.dumps({"seed": seed, "N": N, "dims": dims, "nnz": nnz, "alpha": alpha,
+                                 "R": R}))
+        print(f"tensor {k} N={N} R={R} nnz={nnz} cands={len(cands)} ms={np.round(ms, 3).tolist()} "
               f"analytic={chosen}", flush=True)
     np.savez(args.out, X=np.array(rows, dtype=np.float32), y=np.array(labels, dtype=np.float32),
              tensor=np.array(tid), cand=np.array(cidx), analytic=np.array(analytic),
@@ -115,13 +121,31 @@ def regrets(y, tensor, cand, analytic, pred, ids):
             for k, v in out.items()}
 
 
+def load_sets(paths):
+    """Union of data sets; tensor ids offset per set. Returns the arrays and
+    a held-out mask per tensor (the last 20% of every set)."""
+    Xs, ys, ts, cs, an, held = [], [], [], [], [], []
+    off = 0
+    for p in paths:
+        z = np.load(p)
+        nt = len(z["analytic"])
+        split = int(round(nt * 0.8))
+        Xs.append(z["X"])
+        ys.append(z["y"])
+        ts.append(z["tensor"] + off)
+        cs.append(z["cand"])
+        an.append(z["analytic"])
+        held += [k >= split for k in range(nt)]
+        off += nt
+    return (np.concatenate(Xs), np.concatenate(ys), np.concatenate(ts), np.concatenate(cs),
+            np.concatenate(an), np.array(held))
+
+
 def train(args):
     A.lib().adatm_set_device(0)
-    z = np.load(args.data)
-    X, y, tensor, cand, analytic = z["X"], z["y"], z["tensor"], z["cand"], z["analytic"]
-    nt = int(tensor.max()) + 1
-    split = int(round(nt * 0.8))
-    tr = tensor < split
+    X, y, tensor, cand, analytic, held_t = load_sets(args.data)
+    nt = len(analytic)
+    tr = ~held_t[tensor]
     mean = X[tr].mean(axis=0)
     std = X[tr].std(axis=0)
     std[std < 1e-6] = 1.0
@@ -130,12 +154,12 @@ def train(args):
     loss = net.train(Xs[tr], y[tr], epochs=args.epochs, batch=args.batch, lr=args.lr, seed=args.seed)
     model = A.PlanModel(WIDTHS, net.get_params(), mean, std)
     pred = model.predict(X)
-    held = list(range(split, nt))
+    held = [k for k in range(nt) if held_t[k]]
     rg = regrets(y, tensor, cand, analytic, pred, held)
-    rg_train = regrets(y, tensor, cand, analytic, pred, list(range(split)))
+    rg_train = regrets(y, tensor, cand, analytic, pred, [k for k in range(nt) if not held_t[k]])
     report = {"train_loss": loss, "rows": int(len(y)), "tensors": nt, "held_out_tensors": len(held),
-              "held_out": rg, "train": rg_train}
-    model.save(args.model, report=json.dumps(report), split=split)
+              "held_out": rg, "train": rg_train, "data": [os.path.basename(p) for p in args.data]}
+    model.save(args.model, report=json.dumps(report), held=held_t)
     print(json.dumps(report, indent=1))
 
 
@@ -150,7 +174,7 @@ def evaluate(args):
     if args.big:
         t = A.Tensor.generate(BIG_DIMS, BIG_NNZ, alpha=BIG_ALPHA, seed=2026)
     else:
-        N, dims, nnz, alpha = draw_tensor_spec(args.seed, args.max_nnz)
+        N, dims, nnz, alpha, _ = draw_tensor_spec(args.seed, args.max_nnz)
         t = A.Tensor.generate(dims, nnz, alpha=alpha, seed=args.seed)
     X, nbytes, cands, ms, chosen = measure_tensor(t, args.sweeps)
     _, learned, used = A.plan_learned(t, RANK, model)
@@ -171,10 +195,13 @@ def main():
     m.add_argument("--tensors", type=int, default=400)
     m.add_argument("--seed0", type=int, default=1000)
     m.add_argument("--max-nnz", type=float, default=4e6)
+    m.add_argument("--min-nnz", type=float, default=1e5)
+    m.add_argument("--min-order", type=int, default=4)
+    m.add_argument("--ranks", default=str(RANK))
     m.add_argument("--sweeps", type=int, default=5)
     m.add_argument("--out", required=True)
     t = sub.add_parser("train")
-    t.add_argument("--data", required=True)
+    t.add_argument("--data", action="append", required=True)
     t.add_argument("--model", default=DEFAULT_MODEL)
     t.add_argument("--epochs", type=int, default=400)
     t.add_argument("--batch", type=int, default=128)
