@@ -450,14 +450,20 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
 // levels above the parent (it changes only where a unit closes two or more
 // levels). Units are independent, so a warp takes 32 / W of them per step:
 // W lanes per unit, 4 columns (one float4) per lane, vector atomics.
+// Skewed modes send many units of a batch to the same output row, and the
+// vector atomics on that row serialise; so a batch whose units repeat an
+// output row first stages every unit's row in shared memory and lets the
+// first unit of each repeated row add the group's sum with one atomic.
 // ---------------------------------------------------------------------------
-template <int W>
-constexpr size_t scatter_warp_smem() {
-  return (size_t)kMaxModes * 128 * sizeof(float) + kBatch * (sizeof(uint2) + sizeof(uint32_t));
-}
-template <int W>
-constexpr size_t scatter_smem() {
-  return (size_t)kWarps * scatter_warp_smem<W>();
+__device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ void sts4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+
+// Per-warp shared memory: prefix rows (kMaxModes x 128), the batch's (id,
+// value) pairs, parent ids, output-row groups and leaders, then the staged
+// unit rows (kBatch x ldr).
+__host__ __device__ constexpr size_t scatter_warp_bytes(int ldr) {
+  return ((size_t)kMaxModes * 128 * sizeof(float) + kBatch * (sizeof(uint2) + 3 * sizeof(uint32_t)) +
+          (size_t)kBatch * ldr * sizeof(float) + 15) / 16 * 16;
 }
 
 template <FactorType FT>
@@ -492,10 +498,13 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t chunk_id = blockIdx.x * kWarps + warp;
   if (chunk_id >= a.nchunks) return;
-  unsigned char *wbase = walk_raw + (size_t)warp * scatter_warp_smem<W>();
+  unsigned char *wbase = walk_raw + (size_t)warp * scatter_warp_bytes(a.ldr);
   float *preq = reinterpret_cast<float *>(wbase);  // kMaxModes x 128 columns
   uint2 *ustage = reinterpret_cast<uint2 *>(preq + kMaxModes * 128);
   uint32_t *pstage = reinterpret_cast<uint32_t *>(ustage + kBatch);
+  uint32_t *gstage = pstage + kBatch;  // lanes sharing each unit's output row
+  uint32_t *lstage = gstage + kBatch;  // units that lead a repeated row
+  float *xs = reinterpret_cast<float *>(lstage + kBatch);  // staged unit rows
   const int slot = lane / W;
   const int col = 4 * (lane % W);
   const bool act = col < a.R;
@@ -521,6 +530,11 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
     if (d >= 1 && (uint64_t)nodeP + lane < a.nfibs[d - 1]) pf = __ldg(a.fids[d - 1] + nodeP + lane);
     ustage[lane] = make_uint2(id, __float_as_uint(v));
     pstage[lane] = pf;
+    // units of this batch that repeat an output row
+    const uint32_t grp = __match_any_sync(~0u, in ? id : 0xFFFFFFFFu);
+    const bool lead = in && (grp & lanemask_lt()) == 0;
+    const bool stage = __ballot_sync(~0u, in && !lead) != 0u;
+    gstage[lane] = grp;
     __syncwarp();
     int k = 0;
     while (k < cnt) {
@@ -547,7 +561,10 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
           const fv<4> m = ld_rows<4>(a.src_rows, base + (unit & 31), a.ldr, col, ok);
           x = make_float4(m.x[0] * p.x, m.x[1] * p.y, m.x[2] * p.z, m.x[3] * p.w);
         }
-        if (ok) atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)e.x * a.ldr + col), x);
+        if (ok) {
+          if (stage) sts4(xs + (unit & 31) * a.ldr + col, x);
+          else atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)e.x * a.ldr + col), x);
+        }
       }
       if (deep == ke) {
         // unit ke closes levels d-1 .. d-c (c >= 2): the levels above its
@@ -559,6 +576,29 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
         __syncwarp();
       }
       k = ke + 1;
+    }
+    if (stage) {
+      // one atomic per distinct output row: the leading unit sums its group
+      __syncwarp();
+      const uint32_t L = __ballot_sync(~0u, lead);
+      if (lead) lstage[__popc(L & lanemask_lt())] = (uint32_t)lane;
+      __syncwarp();
+      const int nl = __popc(L);
+      for (int i0 = 0; i0 < nl; i0 += UPS) {
+        const int i = i0 + slot;
+        if (i < nl && act) {
+          const uint32_t u = lstage[i];
+          uint32_t members = gstage[u];
+          float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+          while (members) {
+            const int m = __ffs(members) - 1;
+            members &= members - 1u;
+            const float4 x = lds4(xs + m * a.ldr + col);
+            sum = make_float4(sum.x + x.x, sum.y + x.y, sum.z + x.z, sum.w + x.w);
+          }
+          atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)ustage[u].x * a.ldr + col), sum);
+        }
+      }
     }
     if (d >= 1 && lane == d - 1) nodeL += (uint32_t)__popc(M);
     __syncwarp();
@@ -651,10 +691,10 @@ void launch_contract(int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s
 template <FactorType FT, bool LEAF>
 void launch_scatter(int w, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
   switch (w) {
-    case 4: k_scatter<4, FT, LEAF><<<blocks, 256, scatter_smem<4>(), s>>>(a); break;
-    case 8: k_scatter<8, FT, LEAF><<<blocks, 256, scatter_smem<8>(), s>>>(a); break;
-    case 16: k_scatter<16, FT, LEAF><<<blocks, 256, scatter_smem<16>(), s>>>(a); break;
-    case 32: k_scatter<32, FT, LEAF><<<blocks, 256, scatter_smem<32>(), s>>>(a); break;
+    case 4: k_scatter<4, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
+    case 8: k_scatter<8, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
+    case 16: k_scatter<16, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
+    case 32: k_scatter<32, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
     default: throw BadInput("unsupported lanes per unit");
   }
   ADATM_LAUNCH();
@@ -689,7 +729,7 @@ void set_walk_attributes() {
 #define ADATM_ATTR_S(W, FT, LEAF)                                                 \
   ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF>,                         \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                  (int)scatter_smem<W>()));
+                                  (int)(kWarps * scatter_warp_bytes(128))));
 #define ADATM_ATTR_ALL(M, X)                \
   M(X, FactorType::F32, true)               \
   M(X, FactorType::F32, false)              \
