@@ -458,11 +458,11 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 __device__ __forceinline__ void sts4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 
-// Per-warp shared memory: prefix rows (kMaxModes x 128), the batch's (id,
-// value) pairs, parent ids, output-row groups and leaders, then the staged
-// unit rows (kBatch x ldr).
+// Per-warp shared memory, sized by the row width: prefix rows (kMaxModes x
+// ldr), the batch's (id, value) pairs, parent ids, output-row groups and
+// leaders, then the staged unit rows (kBatch x ldr).
 __host__ __device__ constexpr size_t scatter_warp_bytes(int ldr) {
-  return ((size_t)kMaxModes * 128 * sizeof(float) + kBatch * (sizeof(uint2) + 3 * sizeof(uint32_t)) +
+  return ((size_t)kMaxModes * ldr * sizeof(float) + kBatch * (sizeof(uint2) + 3 * sizeof(uint32_t)) +
           (size_t)kBatch * ldr * sizeof(float) + 15) / 16 * 16;
 }
 
@@ -472,7 +472,8 @@ __device__ __forceinline__ float4 ld_factor4(const void *U, uint32_t row, int ld
   return make_float4(r.x[0], r.x[1], r.x[2], r.x[3]);
 }
 
-// Prefix rows (per column, all ldr columns) of levels lo..hi-1.
+// Prefix rows (per column, all ldr columns; rows ldr floats apart) of levels
+// lo..hi-1.
 template <FactorType FT>
 __device__ __noinline__ void scatter_prefix(const WalkArgs &a, float *preq, uint32_t nodeL, int lo,
                                             int hi, int lane) {
@@ -484,10 +485,10 @@ __device__ __noinline__ void scatter_prefix(const WalkArgs &a, float *preq, uint
     const uint32_t f = valid ? __ldg(a.fids[l] + n) : 0u;
     float4 row = ld_factor4<FT>(a.U[l], f, a.ldr, c, act && valid);
     if (l > 0 && act) {
-      const float4 p = *reinterpret_cast<const float4 *>(preq + (l - 1) * 128 + c);
+      const float4 p = *reinterpret_cast<const float4 *>(preq + (l - 1) * a.ldr + c);
       row = make_float4(row.x * p.x, row.y * p.y, row.z * p.z, row.w * p.w);
     }
-    if (act) *reinterpret_cast<float4 *>(preq + l * 128 + c) = row;
+    if (act) *reinterpret_cast<float4 *>(preq + l * a.ldr + c) = row;
   }
 }
 
@@ -499,8 +500,8 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
   const uint32_t chunk_id = blockIdx.x * kWarps + warp;
   if (chunk_id >= a.nchunks) return;
   unsigned char *wbase = walk_raw + (size_t)warp * scatter_warp_bytes(a.ldr);
-  float *preq = reinterpret_cast<float *>(wbase);  // kMaxModes x 128 columns
-  uint2 *ustage = reinterpret_cast<uint2 *>(preq + kMaxModes * 128);
+  float *preq = reinterpret_cast<float *>(wbase);  // kMaxModes x ldr columns
+  uint2 *ustage = reinterpret_cast<uint2 *>(preq + kMaxModes * a.ldr);
   uint32_t *pstage = reinterpret_cast<uint32_t *>(ustage + kBatch);
   uint32_t *gstage = pstage + kBatch;  // lanes sharing each unit's output row
   uint32_t *lstage = gstage + kBatch;  // units that lead a repeated row
@@ -542,7 +543,7 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
       const int deep = rest ? __ffs(rest) - 1 : 32;
       const int ke = min(deep, cnt - 1);
       float4 Q = make_float4(1.f, 1.f, 1.f, 1.f);
-      if (d >= 2 && act) Q = *reinterpret_cast<const float4 *>(preq + (d - 2) * 128 + col);
+      if (d >= 2 && act) Q = *reinterpret_cast<const float4 *>(preq + (d - 2) * a.ldr + col);
       for (int k0 = k; k0 <= ke; k0 += UPS) {
         const int unit = k0 + slot;
         const bool ok = unit <= ke && act;
