@@ -328,6 +328,34 @@ def cpd_als_iterate_adaptive(csf: CsfSet, rcsf: RcsfSet, groups, use_csfs, use_t
     return {"fit": fit, "lambda": lam, "factors": keep}
 
 
+class CpdIterator:
+    """Repeated cpd_als_iterate_adaptive calls on the same host factor
+    buffers, as a C caller makes them: the matrix_t array is built once and
+    the library updates the factors in place (host FP64 in, host FP64 out)."""
+
+    def __init__(self, csf: CsfSet, rcsf: RcsfSet, groups, use_csfs, use_tags, mats, opts=None):
+        self.csf, self.rcsf = csf, rcsf
+        self.opts = (csf.opts if opts is None else np.ascontiguousarray(opts, np.float64)).copy()
+        self.R = mats[0].shape[1]
+        self.arr, self.factors, self._out, self._s1, self._s2 = _matrix_array(
+            [np.array(m, dtype=np.float64, order="C", copy=True) for m in mats],
+            max(m.shape[0] for m in mats), self.R)
+        self.lam = np.zeros(self.R)
+        self._ga = _GroupArray(groups, len(mats))
+        self._uc, self._ucp = _u64(use_csfs)
+        self._ut, self._utp = _u64(use_tags)
+        self._lamp = self.lam.ctypes.data_as(C.POINTER(C.c_double))
+        self._optp = self.opts.ctypes.data_as(C.POINTER(C.c_double))
+
+    def step(self, niters=1, tol=0.0):
+        self.opts[OPT_NITER] = niters
+        self.opts[OPT_TOLERANCE] = tol
+        return lib().cpd_als_iterate_adaptive(self.csf.ptr, self.rcsf.ptr if self.rcsf else None,
+                                              len(self.csf), self._ga.arr, self._ga.n, self._ucp,
+                                              self._utp, self.arr, self._lamp, self.R, None,
+                                              self._optp)
+
+
 # ---------------------------------------------------------------------------
 # device-resident interface
 # ---------------------------------------------------------------------------

@@ -473,10 +473,10 @@ void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, 
 
 void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s) {
   const int blocks = 256;
-  DevBuf<double> part(blocks);
-  k_frob_partial<<<blocks, kFrobThreads, 0, s>>>(vals, n, part.get());
+  if (w.frob_part.n < (size_t)blocks) w.frob_part.alloc(blocks);
+  k_frob_partial<<<blocks, kFrobThreads, 0, s>>>(vals, n, w.frob_part.get());
   ADATM_LAUNCH();
-  k_frob_final<<<1, 32, 0, s>>>(part.get(), blocks, w.scalars.get());
+  k_frob_final<<<1, 32, 0, s>>>(w.frob_part.get(), blocks, w.scalars.get());
   ADATM_LAUNCH();
   ADATM_CUDA(cudaStreamSynchronize(s));
 }

@@ -20,6 +20,7 @@ struct AlsWork {
   DevBuf<double> scalars;                // [0] ttnormsq, [1] fit, [2] norm, [3] inner
   DevBuf<int> iter;                      // ALS iteration counter (device)
   DevBuf<double> fit_trace;              // per-iteration fits
+  DevBuf<double> frob_part;              // partial sums of ||X||^2
   int max_trace = 0;
   void init(int nmodes_, int R_, int nblocks_, int max_iters);
 };

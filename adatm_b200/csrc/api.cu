@@ -210,24 +210,12 @@ void check_plan(const Plan &p) {
   }
 }
 
-void post_process(int N, const uint64_t *dims, uint64_t R, double *const *mats, double *lambda) {
-  // cpd_post_process: 2-normalise every factor, lambda absorbs the norms
-  std::vector<double> nrm(R);
-  for (int m = 0; m < N; ++m) {
-    std::fill(nrm.begin(), nrm.end(), 0.0);
-    for (uint64_t i = 0; i < dims[m]; ++i)
-      for (uint64_t r = 0; r < R; ++r) nrm[r] += mats[m][i * R + r] * mats[m][i * R + r];
-    for (uint64_t r = 0; r < R; ++r) nrm[r] = std::sqrt(nrm[r]);
-    for (uint64_t i = 0; i < dims[m]; ++i)
-      for (uint64_t r = 0; r < R; ++r) mats[m][i * R + r] /= nrm[r];
-    for (uint64_t r = 0; r < R; ++r) lambda[r] *= nrm[r];
-  }
-}
 
 // The ALS loop shared by the splatt_* entry points, with the reference's
 // per-iteration report (adatm_cpd.c:343-354).
 double run_als(Engine &e, uint64_t niters, double tol, int verbosity) {
   e.als_begin();
+  e.capture_graph();  // one sweep as a CUDA graph, reused across calls
   double fit = 0, old = 0;
   const auto t0 = std::chrono::steady_clock::now();
   for (uint64_t it = 0; it < niters; ++it) {
@@ -261,9 +249,7 @@ void fill_kruskal(Engine &e, double fit, splatt_kruskal *k) {
     k->factors[m] = (double *)malloc((size_t)e.dims()[m] * R * sizeof(double));
     mats[m] = k->factors[m];
   }
-  e.get_factors(mats);
-  e.get_lambda(k->lambda);
-  post_process(N, e.dims(), R, mats, k->lambda);
+  e.get_normalized(mats, k->lambda);
 }
 
 void plan_to_c(const Plan &p, adatm_plan *o) {
@@ -769,9 +755,7 @@ double cpd_als_iterate_adaptive(splatt_csf const *const tensors, rcsf_seq_adapti
     e.set_factors(fm);
     fit = run_als(e, (uint64_t)opts[SPLATT_OPTION_NITER], opts[SPLATT_OPTION_TOLERANCE],
                   (int)opts[SPLATT_OPTION_VERBOSITY]);
-    e.get_factors(om);
-    e.get_lambda(lambda);
-    post_process(N, e.dims(), nfactors, om, lambda);
+    e.get_normalized(om, lambda);
   });
   if (rc != SPLATT_SUCCESS) fprintf(stderr, "cpd_als_iterate_adaptive: %s\n", g_last_error.c_str());
   return fit;

@@ -1,5 +1,7 @@
 // engine.cu -- tensor + plan + trees + memo rows + factors + CP-ALS sweep.
 #include <algorithm>
+#include <thread>
+#include <cmath>
 #include <cstring>
 
 #include "engine.hpp"
@@ -7,6 +9,25 @@
 namespace adatm {
 
 namespace {
+// Rows [0, rows) of a host conversion split over a few threads when large.
+template <typename F>
+void host_rows(uint64_t rows, uint64_t row_elems, F &&f) {
+  const uint64_t work = rows * row_elems;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned nt = (unsigned)std::min<uint64_t>({(uint64_t)std::min(hw, 8u), work / 65536 + 1, rows});
+  if (nt <= 1) {
+    f(0, rows);
+    return;
+  }
+  std::vector<std::thread> ts;
+  const uint64_t step = (rows + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const uint64_t a = t * step, b = std::min(rows, a + step);
+    if (a < b) ts.emplace_back([&f, a, b] { f(a, b); });
+  }
+  for (auto &th : ts) th.join();
+}
+
 int depth_of(const DevCsf &c, int mode) {
   for (int l = 0; l < c.nmodes; ++l)
     if ((int)c.dim_perm[l] == mode) return l;
@@ -55,12 +76,18 @@ Engine::Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<De
     ADATM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   }
   w_.init(N, (int)R_, 2 * sms, opt_.max_iters);
+  ADATM_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
+  ADATM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
+  ADATM_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
   build_walks();
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
 Engine::~Engine() {
   drop_graph();
+  if (join_) cudaEventDestroy(join_);
+  if (fork_) cudaEventDestroy(fork_);
+  if (side_) cudaStreamDestroy(side_);
   if (staging_) cudaFreeHost(staging_);
 }
 
@@ -325,10 +352,14 @@ void Engine::set_factors(const double *const *host) {
   for (int m = 0; m < coo_->nmodes; ++m) {
     const uint64_t I = coo_->dims[m];
     float *b = buf + off;
-    for (uint64_t i = 0; i < I; ++i) {
-      for (uint64_t r = 0; r < R_; ++r) b[i * ldr_ + r] = (float)host[m][i * R_ + r];
-      for (uint64_t r = R_; r < (uint64_t)ldr_; ++r) b[i * ldr_ + r] = 0.f;
-    }
+    const double *h = host[m];
+    const uint64_t R = R_, L = (uint64_t)ldr_;
+    host_rows(I, L, [=](uint64_t i0, uint64_t i1) {
+      for (uint64_t i = i0; i < i1; ++i) {
+        for (uint64_t r = 0; r < R; ++r) b[i * L + r] = (float)h[i * R + r];
+        for (uint64_t r = R; r < L; ++r) b[i * L + r] = 0.f;
+      }
+    });
     ADATM_CUDA(cudaMemcpyAsync(A_[m].get(), b, (size_t)I * ldr_ * sizeof(float),
                                cudaMemcpyHostToDevice, stream_));
     if (Ab_[m].get()) to_bf16(A_[m].get(), Ab_[m].get(), I, ldr_, stream_);
@@ -357,6 +388,45 @@ void Engine::get_factors(double *const *host) {
   }
 }
 
+void Engine::get_normalized(double *const *host, double *lambda) {
+  const int N = coo_->nmodes;
+  size_t total = 0;
+  for (int m = 0; m < N; ++m) total += (size_t)coo_->dims[m] * ldr_;
+  float *buf = staging(total);
+  std::vector<double> diag((size_t)N * R_ * R_);
+  size_t off = 0;
+  for (int m = 0; m < N; ++m) {
+    ADATM_CUDA(cudaMemcpyAsync(buf + off, A_[m].get(), (size_t)coo_->dims[m] * ldr_ * sizeof(float),
+                               cudaMemcpyDeviceToHost, stream_));
+    ADATM_CUDA(cudaMemcpyAsync(diag.data() + (size_t)m * R_ * R_, G_[m].get(),
+                               R_ * R_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    off += (size_t)coo_->dims[m] * ldr_;
+  }
+  ADATM_CUDA(cudaMemcpyAsync(lambda, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost,
+                             stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  std::vector<double> inv(R_);
+  off = 0;
+  for (int m = 0; m < N; ++m) {
+    const double *G = diag.data() + (size_t)m * R_ * R_;
+    for (uint64_t r = 0; r < R_; ++r) {
+      const double nrm = std::sqrt(std::max(G[r * R_ + r], 0.0));
+      inv[r] = nrm > 0 ? 1.0 / nrm : 0.0;
+      lambda[r] *= nrm;
+    }
+    const uint64_t I = coo_->dims[m];
+    const float *b = buf + off;
+    double *h = host[m];
+    const double *iv = inv.data();
+    const uint64_t R = R_, L = (uint64_t)ldr_;
+    host_rows(I, R, [=](uint64_t i0, uint64_t i1) {
+      for (uint64_t i = i0; i < i1; ++i)
+        for (uint64_t r = 0; r < R; ++r) h[i * R + r] = (double)b[i * L + r] * iv[r];
+    });
+    off += (size_t)I * ldr_;
+  }
+}
+
 void Engine::get_lambda(double *host) const {
   ADATM_CUDA(cudaMemcpyAsync(host, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost,
                              stream_));
@@ -366,7 +436,10 @@ void Engine::get_lambda(double *host) const {
 void Engine::als_begin() {
   for (int m = 0; m < coo_->nmodes; ++m)
     gram(A_[m].get(), coo_->dims[m], (int)R_, ldr_, G_[m].get(), w_, stream_);
-  frob_sq(csf_[0]->vals64.get(), coo_->nnz, w_, stream_);
+  if (!ttnorm_ready_) {
+    frob_sq(csf_[0]->vals64.get(), coo_->nnz, w_, stream_);
+    ttnorm_ready_ = true;
+  }
   ADATM_CUDA(cudaMemsetAsync(w_.iter.get(), 0, sizeof(int), stream_));
   ADATM_CUDA(cudaMemsetAsync(w_.fit_trace.get(), 0, w_.max_trace * sizeof(double), stream_));
   ADATM_CUDA(cudaStreamSynchronize(stream_));
@@ -377,8 +450,14 @@ void Engine::sweep_eager() {
   GramSet gs;
   for (int m = 0; m < kMaxModes; ++m) gs.G[m] = m < N ? G_[m].get() : nullptr;
   for (int m = 0; m < N; ++m) {
+    // the Gram inverse of mode m needs only the other modes' Grams, final
+    // since mode m-1's update: it runs beside mode m's MTTKRP
+    ADATM_CUDA(cudaEventRecord(fork_, stream_));
+    ADATM_CUDA(cudaStreamWaitEvent(side_, fork_, 0));
+    gram_inverse(gs, m, w_, side_);
+    ADATM_CUDA(cudaEventRecord(join_, side_));
     mttkrp_as(m, M_.get(), sweep_type(m));
-    gram_inverse(gs, m, w_, stream_);
+    ADATM_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
     update_factor(M_.get(), coo_->dims[m], A_[m].get(), Ab_[m].get(), G_[m].get(), m == N - 1, w_,
                   stream_);
   }

@@ -50,6 +50,11 @@ class Engine {
   void set_factors(const double *const *host);          // dims[m] x R each
   void get_factors(double *const *host);
   void get_lambda(double *host) const;
+  // The factors as the reference returns them after cpd_post_process: every
+  // column scaled to unit 2-norm (norms from the device Grams' diagonals,
+  // which the sweep keeps current), lambda multiplied by those norms; one
+  // pass over the downloaded rows.
+  void get_normalized(double *const *host, double *lambda);
   float *factor(int m) { return A_[m].get(); }
 
   // MTTKRP of `mode` following the plan (tags 0/1/2) into out (dims x ldr,
@@ -108,12 +113,17 @@ class Engine {
   DevBuf<double> G_[kMaxModes];
   DevBuf<float> M_;
   AlsWork w_;
+  bool ttnorm_ready_ = false;    // ||X||^2 computed (the tensor never changes)
   float *staging_ = nullptr;     // pinned host rows for factor transfers
   size_t staging_n_ = 0;
   float *staging(size_t n);
   cudaGraph_t graph_ = nullptr;
   cudaGraphExec_t graph_exec_ = nullptr;
   void drop_graph();
+  // Side stream for the Gram inverse of a mode, which overlaps that mode's
+  // MTTKRP (it reads only the other modes' Grams); fork / join events.
+  cudaStream_t side_ = nullptr;
+  cudaEvent_t fork_ = nullptr, join_ = nullptr;
 };
 
 // Many independent tensors swept together: one CUDA graph holds one ALS

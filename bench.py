@@ -351,15 +351,15 @@ def run_ours(args):
     cs = A.csf_alloc_adaptive(inds, vals, dims, groups)
     rs = A.rcsf_alloc_adaptive(cs, RANK, groups)
     uc, ut = A.decide_use_csfs(nmodes, groups, len(cs))
-    import oracle as O
-    mats = O.init_factors(dims, RANK, SEED)
-    A.cpd_als_iterate_adaptive(cs, rs, groups, uc, ut, mats, 1, 0.0)
+    rng = np.random.default_rng(SEED)
+    mats = [rng.random((d, RANK)) for d in dims]
+    it = A.CpdIterator(cs, rs, groups, uc, ut, mats)
+    it.step(1)
     E = max(3, min(K, 20))
     barrier(world)
     te = time.perf_counter()
     for _ in range(E):
-        r = A.cpd_als_iterate_adaptive(cs, rs, groups, uc, ut, mats, 1, 0.0)
-        mats = r["factors"]
+        it.step(1)  # factors in and out of the same host buffers
     e2e_s = max_over_ranks(time.perf_counter() - te, world)
     ldr = (RANK + 3) // 4 * 4
     h2d = sum(dims) * ldr * 4
