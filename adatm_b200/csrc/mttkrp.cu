@@ -24,6 +24,7 @@ struct WalkArgs {
   float *store[kMaxModes];
   float *out;
   const uint32_t *sched;
+  uint32_t *counter;           // chunks claimed so far (zeroed before each launch)
 };
 
 // ---------------------------------------------------------------------------
@@ -224,19 +225,18 @@ struct RowSrc {
   }
 };
 
-// Shared memory of one contraction warp: kBatch item rows, a carry row per
-// level (the open node's partial sum) and a prefix row per level (P_l = U_0
-// [node_0] * ... * U_l[node_l] for the levels above d), all in fv<V> slots of
-// 32 lanes; then the batch's (id, value) pairs and a 32-word exchange buffer.
-constexpr int kSlots = kBatch + 2 * kMaxModes;
-
+// Shared memory of one contraction warp: kBatch item rows and one row per
+// level 0..N-2 -- the prefix P_l = U_0[node_0] * ... * U_l[node_l] for l < d,
+// the open node's partial sum (carry) for d <= l < S; the two ranges never
+// overlap -- all in fv<V> slots of 32 lanes; then the batch's (id, value)
+// pairs and a 32-word exchange buffer.
 template <int V>
-constexpr size_t contract_warp_smem() {
-  return (size_t)kSlots * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint2) + sizeof(uint32_t));
+__host__ __device__ constexpr size_t contract_warp_smem(int N) {
+  return (size_t)(kBatch + N - 1) * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint2) + sizeof(uint32_t));
 }
 template <int V>
-constexpr size_t contract_smem() {
-  return (size_t)kWarps * contract_warp_smem<V>();
+constexpr size_t contract_smem(int N) {
+  return (size_t)kWarps * contract_warp_smem<V>(N);
 }
 
 // Recompute the prefix rows of levels lo..hi-1 from the node indices (lane l
@@ -292,155 +292,162 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     k_contract(const __grid_constant__ WalkArgs a) {
   extern __shared__ __align__(16) unsigned char walk_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t chunk_id = blockIdx.x * kWarps + warp;
-  if (chunk_id >= a.nchunks) return;
-  unsigned char *wbase = walk_raw + (size_t)warp * contract_warp_smem<V>();
+  unsigned char *wbase = walk_raw + (size_t)warp * contract_warp_smem<V>(a.N);
   fv<V> *items = reinterpret_cast<fv<V> *>(wbase);
-  fv<V> *carry = items + kBatch * 32;
-  fv<V> *pre = carry + kMaxModes * 32;
-  uint2 *ustage = reinterpret_cast<uint2 *>(pre + kMaxModes * 32);
+  fv<V> *carry = items + kBatch * 32;  // rows d..S-1
+  fv<V> *pre = carry;                  // rows 0..d-1
+  uint2 *ustage = reinterpret_cast<uint2 *>(carry + (a.N - 1) * 32);
   uint32_t *xbuf = reinterpret_cast<uint32_t *>(ustage + kBatch);
   const int col = lane * V;
   const bool act = col < a.R;
   const int S = a.S, d = a.d;
-  const uint32_t *sc = a.sched + (size_t)chunk_id * (S + 1);
-  uint32_t nodeL = lane < S ? sc[lane] : 0u;
-  uint32_t part = sc[S];
-  uint32_t touched = 0;
-  for (int l = d; l < S - 1; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
-  if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
-  const RowSrc<V, FT> Us(a.U_src, a.ldr, col, act);
-  fv<V> acc = fv_fill<V>(0.f);  // open node of level S-1
-  constexpr int SB = 16 / V;    // unit rows in flight per lane
-  const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
-  const uint64_t u1 = min(u0 + a.chunk, a.nunits);
-  for (uint64_t base = u0; base < u1; base += kBatch) {
-    const int cnt = (int)min((uint64_t)kBatch, u1 - base);
-    const bool in = lane < cnt;
-    const uint32_t id = in ? __ldg(a.src_ids + base + lane) : 0u;
-    float v = 0.f;
-    if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
-    const uint32_t cd = in ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
-    const uint32_t M = __ballot_sync(~0u, cd >= 1u);
-    ustage[lane] = make_uint2(id, __float_as_uint(v));
-    __syncwarp();
-    int j = 0;
-    auto run = [&](auto full) {
-      constexpr bool FULL = decltype(full)::value;
-#pragma unroll
-      for (int k0 = 0; k0 < kBatch; k0 += SB) {
-        if (!FULL && k0 >= cnt) break;
-        fv<V> g[SB];
-        fv<V> m[LEAF ? 1 : SB];
-        float vv[LEAF ? SB : 1];
-#pragma unroll
-        for (int q = 0; q < SB; ++q) {
-          const int k = k0 + q;
-          // lanes past the rank read column 0 through Us's base, so only
-          // the units past the batch need the row-0 substitute
-          const bool ok = FULL || k < cnt;
-          const uint2 e = ustage[k];
-          g[q] = Us.load(e.x, ok);
-          if constexpr (LEAF) vv[q] = __uint_as_float(e.y);
-          if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok && act);
-        }
-#pragma unroll
-        for (int q = 0; q < SB; ++q) {
-          const int k = k0 + q;
-          if (FULL || k < cnt) {
-            if constexpr (LEAF) fv_axpy(acc, vv[LEAF ? q : 0], g[q]);
-            else fv_fma(acc, m[LEAF ? 0 : q], g[q]);
-            if ((M >> k) & 1u) {
-              items[j * 32 + lane] = acc;
-              acc = fv_fill<V>(0.f);
-              ++j;
+  // a resident grid: each warp claims chunks from a counter, the next one
+  // while it walks the current one
+  uint32_t claim = lane == 0 ? atomicAdd(a.counter, 1u) : 0u;
+  uint32_t chunk_id = __shfl_sync(~0u, claim, 0);
+  while (chunk_id < a.nchunks) {
+    claim = lane == 0 ? atomicAdd(a.counter, 1u) : 0u;
+    const uint32_t *sc = a.sched + (size_t)chunk_id * (S + 1);
+    uint32_t nodeL = lane < S ? sc[lane] : 0u;
+    uint32_t part = sc[S];
+    uint32_t touched = 0;
+    for (int l = d; l < S - 1; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
+    if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
+    const RowSrc<V, FT> Us(a.U_src, a.ldr, col, act);
+    fv<V> acc = fv_fill<V>(0.f);  // open node of level S-1
+    constexpr int SB = 16 / V;    // unit rows in flight per lane
+    const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
+    const uint64_t u1 = min(u0 + a.chunk, a.nunits);
+    for (uint64_t base = u0; base < u1; base += kBatch) {
+      const int cnt = (int)min((uint64_t)kBatch, u1 - base);
+      const bool in = lane < cnt;
+      const uint32_t id = in ? __ldg(a.src_ids + base + lane) : 0u;
+      float v = 0.f;
+      if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
+      const uint32_t cd = in ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
+      const uint32_t M = __ballot_sync(~0u, cd >= 1u);
+      ustage[lane] = make_uint2(id, __float_as_uint(v));
+      __syncwarp();
+      int j = 0;
+      auto run = [&](auto full) {
+        constexpr bool FULL = decltype(full)::value;
+  #pragma unroll
+        for (int k0 = 0; k0 < kBatch; k0 += SB) {
+          if (!FULL && k0 >= cnt) break;
+          fv<V> g[SB];
+          fv<V> m[LEAF ? 1 : SB];
+          float vv[LEAF ? SB : 1];
+  #pragma unroll
+          for (int q = 0; q < SB; ++q) {
+            const int k = k0 + q;
+            // lanes past the rank read column 0 through Us's base, so only
+            // the units past the batch need the row-0 substitute
+            const bool ok = FULL || k < cnt;
+            const uint2 e = ustage[k];
+            g[q] = Us.load(e.x, ok);
+            if constexpr (LEAF) vv[q] = __uint_as_float(e.y);
+            if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok && act);
+          }
+  #pragma unroll
+          for (int q = 0; q < SB; ++q) {
+            const int k = k0 + q;
+            if (FULL || k < cnt) {
+              if constexpr (LEAF) fv_axpy(acc, vv[LEAF ? q : 0], g[q]);
+              else fv_fma(acc, m[LEAF ? 0 : q], g[q]);
+              if ((M >> k) & 1u) {
+                items[j * 32 + lane] = acc;
+                acc = fv_fill<V>(0.f);
+                ++j;
+              }
             }
           }
         }
-      }
-    };
-    if (cnt == kBatch) run(std::true_type{});
-    else run(std::false_type{});
-    if ((M >> (cnt - 1)) & 1u) touched &= ~(1u << (S - 1));
-    else touched |= 1u << (S - 1);
-    int n = __popc(M);
-    uint32_t icd = compact_bits(M, cd - 1u, xbuf, lane);
-    // the level loop: items of level l (node sums that closed in this batch)
-    for (int l = S - 1; l >= d && n > 0; --l) {
-      const uint32_t first = __shfl_sync(~0u, nodeL, l);
-      const bool pfirst = (part >> l) & 1u;
-      const uint32_t fid =
-          (lane < n && (uint64_t)first + lane < a.nfibs[l]) ? __ldg(a.fids[l] + first + lane) : 0u;
-      float *store = a.store[l];
-      if (store != nullptr && (uint64_t)first + n <= a.nfibs[l]) {
-        float *sp = store + (size_t)first * a.ldr + col;
-        if (pfirst) red_rows<V>(sp, 0, 0, 0, items[lane], act);
-        else st_rows<V>(sp, 0, 0, 0, items[lane], act);
-        for (int i = 1; i < n; ++i) {
-          sp += a.ldr;
-          st_rows<V>(sp, 0, 0, 0, items[i * 32 + lane], act);
+      };
+      if (cnt == kBatch) run(std::true_type{});
+      else run(std::false_type{});
+      if ((M >> (cnt - 1)) & 1u) touched &= ~(1u << (S - 1));
+      else touched |= 1u << (S - 1);
+      int n = __popc(M);
+      uint32_t icd = compact_bits(M, cd - 1u, xbuf, lane);
+      // the level loop: items of level l (node sums that closed in this batch)
+      for (int l = S - 1; l >= d && n > 0; --l) {
+        const uint32_t first = __shfl_sync(~0u, nodeL, l);
+        const bool pfirst = (part >> l) & 1u;
+        const uint32_t fid =
+            (lane < n && (uint64_t)first + lane < a.nfibs[l]) ? __ldg(a.fids[l] + first + lane) : 0u;
+        float *store = a.store[l];
+        if (store != nullptr && (uint64_t)first + n <= a.nfibs[l]) {
+          float *sp = store + (size_t)first * a.ldr + col;
+          if (pfirst) red_rows<V>(sp, 0, 0, 0, items[lane], act);
+          else st_rows<V>(sp, 0, 0, 0, items[lane], act);
+          for (int i = 1; i < n; ++i) {
+            sp += a.ldr;
+            st_rows<V>(sp, 0, 0, 0, items[i * 32 + lane], act);
+          }
+        }
+        if (l > d) {
+          const uint32_t Mp = __ballot_sync(~0u, lane < n && icd >= 1u);
+          const RowSrc<V, FT> Ul(a.U[l], a.ldr, col, act);
+          fv<V> cl = carry[(l - 1) * 32 + lane];
+          int jj = 0;
+  #pragma unroll 8
+          for (int i = 0; i < n; ++i) {
+            const fv<V> row = Ul.load(__shfl_sync(~0u, fid, i), true);
+            fv_fma(cl, items[i * 32 + lane], row);
+            if ((Mp >> i) & 1u) {
+              items[jj * 32 + lane] = cl;
+              cl = fv_fill<V>(0.f);
+              ++jj;
+            }
+          }
+          carry[(l - 1) * 32 + lane] = cl;
+          if ((Mp >> (n - 1)) & 1u) touched &= ~(1u << (l - 1));
+          else touched |= 1u << (l - 1);
+          if (lane == l) nodeL += (uint32_t)n;
+          part &= ~(1u << l);
+          icd = compact_bits(Mp, icd - 1u, xbuf, lane);
+          n = __popc(Mp);
+        } else {
+          for (int i = 0; i < n; ++i) {
+            const fv<V> val = items[i * 32 + lane];
+            const uint32_t orow = __shfl_sync(~0u, fid, i);
+            if (d == 0) {
+              if (i == 0 && pfirst) red_rows<V>(a.out, orow, a.ldr, col, val, act);
+              else st_rows<V>(a.out, orow, a.ldr, col, val, act);
+            } else {
+              red_rows<V>(a.out, orow, a.ldr, col, fv_mul(val, pre[(d - 1) * 32 + lane]), act);
+              const uint32_t ci = __shfl_sync(~0u, icd, i);
+              if (ci >= 1u) nodeL = advance_prefix<V, FT>(a, pre, nodeL, d - (int)ci, d, col, act, lane);
+            }
+          }
+          if (lane == l) nodeL += (uint32_t)n;
+          part &= ~(1u << l);
+          n = 0;
         }
       }
+    }
+    // chunk end: the open nodes of levels S-1 .. d add their partial sums
+    carry[(S - 1) * 32 + lane] = acc;
+    for (int l = S - 1; l >= d; --l) {
+      if (!((touched >> l) & 1u)) continue;
+      const uint32_t node = __shfl_sync(~0u, nodeL, l);
+      if ((uint64_t)node >= a.nfibs[l]) continue;
+      const fv<V> val = carry[l * 32 + lane];
+      if (a.store[l] != nullptr) red_rows<V>(a.store[l], node, a.ldr, col, val, act);
       if (l > d) {
-        const uint32_t Mp = __ballot_sync(~0u, lane < n && icd >= 1u);
-        const RowSrc<V, FT> Ul(a.U[l], a.ldr, col, act);
-        fv<V> cl = carry[(l - 1) * 32 + lane];
-        int jj = 0;
-#pragma unroll 8
-        for (int i = 0; i < n; ++i) {
-          const fv<V> row = Ul.load(__shfl_sync(~0u, fid, i), true);
-          fv_fma(cl, items[i * 32 + lane], row);
-          if ((Mp >> i) & 1u) {
-            items[jj * 32 + lane] = cl;
-            cl = fv_fill<V>(0.f);
-            ++jj;
-          }
-        }
-        carry[(l - 1) * 32 + lane] = cl;
-        if ((Mp >> (n - 1)) & 1u) touched &= ~(1u << (l - 1));
-        else touched |= 1u << (l - 1);
-        if (lane == l) nodeL += (uint32_t)n;
-        part &= ~(1u << l);
-        icd = compact_bits(Mp, icd - 1u, xbuf, lane);
-        n = __popc(Mp);
+        const fv<V> r = ld_factor<V, FT>(a.U[l], __ldg(a.fids[l] + node), a.ldr, col, act);
+        fv<V> c2 = carry[(l - 1) * 32 + lane];
+        fv_fma(c2, val, r);
+        carry[(l - 1) * 32 + lane] = c2;
+        touched |= 1u << (l - 1);
       } else {
-        for (int i = 0; i < n; ++i) {
-          const fv<V> val = items[i * 32 + lane];
-          const uint32_t orow = __shfl_sync(~0u, fid, i);
-          if (d == 0) {
-            if (i == 0 && pfirst) red_rows<V>(a.out, orow, a.ldr, col, val, act);
-            else st_rows<V>(a.out, orow, a.ldr, col, val, act);
-          } else {
-            red_rows<V>(a.out, orow, a.ldr, col, fv_mul(val, pre[(d - 1) * 32 + lane]), act);
-            const uint32_t ci = __shfl_sync(~0u, icd, i);
-            if (ci >= 1u) nodeL = advance_prefix<V, FT>(a, pre, nodeL, d - (int)ci, d, col, act, lane);
-          }
-        }
-        if (lane == l) nodeL += (uint32_t)n;
-        part &= ~(1u << l);
-        n = 0;
+        const uint32_t orow = __ldg(a.fids[d] + node);
+        red_rows<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
+                    act);
       }
     }
-  }
-  // chunk end: the open nodes of levels S-1 .. d add their partial sums
-  carry[(S - 1) * 32 + lane] = acc;
-  for (int l = S - 1; l >= d; --l) {
-    if (!((touched >> l) & 1u)) continue;
-    const uint32_t node = __shfl_sync(~0u, nodeL, l);
-    if ((uint64_t)node >= a.nfibs[l]) continue;
-    const fv<V> val = carry[l * 32 + lane];
-    if (a.store[l] != nullptr) red_rows<V>(a.store[l], node, a.ldr, col, val, act);
-    if (l > d) {
-      const fv<V> r = ld_factor<V, FT>(a.U[l], __ldg(a.fids[l] + node), a.ldr, col, act);
-      fv<V> c2 = carry[(l - 1) * 32 + lane];
-      fv_fma(c2, val, r);
-      carry[(l - 1) * 32 + lane] = c2;
-      touched |= 1u << (l - 1);
-    } else {
-      const uint32_t orow = __ldg(a.fids[d] + node);
-      red_rows<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
-                  act);
-    }
+    __syncwarp();
+    chunk_id = __shfl_sync(~0u, claim, 0);
   }
 }
 
@@ -675,15 +682,34 @@ WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   a.U_src = f ? f->U[w.src] : nullptr;
   a.out = out;
   a.sched = w.sched.get();
+  a.counter = w.sched.get() ? w.sched.get() + (size_t)w.nchunks * (w.src + 1) : nullptr;
   return a;
+}
+
+// Blocks of `kernel` that fit on the device at once with `smem` bytes each.
+template <typename K>
+unsigned resident_blocks(K kernel, int threads, size_t smem) {
+  int dev = 0, sms = 0, per_sm = 0;
+  ADATM_CUDA(cudaGetDevice(&dev));
+  ADATM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  ADATM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+  return (unsigned)std::max(1, sms * std::max(1, per_sm));
+}
+
+template <int V, FactorType FT, bool LEAF>
+void launch_contract_v(const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+  const size_t smem = contract_smem<V>(a.N);
+  blocks = std::min(blocks, resident_blocks(k_contract<V, FT, LEAF>, 256, smem));
+  ADATM_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), s));
+  k_contract<V, FT, LEAF><<<blocks, 256, smem, s>>>(a);
 }
 
 template <FactorType FT, bool LEAF>
 void launch_contract(int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
   switch (vec) {
-    case 1: k_contract<1, FT, LEAF><<<blocks, 256, contract_smem<1>(), s>>>(a); break;
-    case 2: k_contract<2, FT, LEAF><<<blocks, 256, contract_smem<2>(), s>>>(a); break;
-    case 4: k_contract<4, FT, LEAF><<<blocks, 256, contract_smem<4>(), s>>>(a); break;
+    case 1: launch_contract_v<1, FT, LEAF>(a, blocks, s); break;
+    case 2: launch_contract_v<2, FT, LEAF>(a, blocks, s); break;
+    case 4: launch_contract_v<4, FT, LEAF>(a, blocks, s); break;
     default: throw BadInput("unsupported columns per lane");
   }
   ADATM_LAUNCH();
@@ -726,7 +752,7 @@ void set_walk_attributes() {
 #define ADATM_ATTR_C(V, FT, LEAF)                                                 \
   ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF>,                        \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                  (int)contract_smem<V>()));
+                                  (int)contract_smem<V>(kMaxModes)));
 #define ADATM_ATTR_S(W, FT, LEAF)                                                 \
   ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF>,                         \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
@@ -756,7 +782,7 @@ void walk_prepare(TreeWalk &w, cudaStream_t s) {
   w.nunits = c.nfibs[w.src];
   if (w.chunk == 0) w.chunk = 32;
   w.nchunks = (uint32_t)((w.nunits + w.chunk - 1) / w.chunk);
-  w.sched.alloc((size_t)std::max<uint32_t>(w.nchunks, 1) * (w.src + 1));
+  w.sched.alloc((size_t)std::max<uint32_t>(w.nchunks, 1) * (w.src + 1) + 1);  // + the chunk counter
   if (w.nchunks == 0) return;
   WalkArgs a = make_args(w, nullptr, nullptr);
   k_schedule<<<(w.nchunks + 255) / 256, 256, 0, s>>>(a, w.sched.get());
