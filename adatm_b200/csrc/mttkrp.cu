@@ -229,10 +229,10 @@ struct RowSrc {
 // level 0..N-2 -- the prefix P_l = U_0[node_0] * ... * U_l[node_l] for l < d,
 // the open node's partial sum (carry) for d <= l < S; the two ranges never
 // overlap -- all in fv<V> slots of 32 lanes; then the batch's (id, value)
-// pairs and a 32-word exchange buffer.
+// (and parent) words and a 32-word exchange buffer.
 template <int V>
 __host__ __device__ constexpr size_t contract_warp_smem(int N) {
-  return (size_t)(kBatch + N - 1) * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint2) + sizeof(uint32_t));
+  return (size_t)(kBatch + N - 1) * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint4) + sizeof(uint32_t));
 }
 template <int V>
 constexpr size_t contract_smem(int N) {
@@ -287,7 +287,13 @@ constexpr int contract_min_blocks() {
   return V == 1 ? 4 : (V == 2 ? 2 : 1);
 }
 
-template <int V, FactorType FT, bool LEAF>
+//
+// FUSE (level S-1 is not stored and lies below d): the nodes of level S-1
+// are not formed. Each unit's product is multiplied by its parent's factor
+// row (U_{S-1} of the level-(S-1) node holding it) and summed straight into
+// the open node of level S-2, so the batch's items are level-(S-2) nodes.
+// The sums equal the unfused ones up to FP32 rounding order.
+template <int V, FactorType FT, bool LEAF, bool FUSE>
 __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     k_contract(const __grid_constant__ WalkArgs a) {
   extern __shared__ __align__(16) unsigned char walk_raw[];
@@ -296,7 +302,7 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
   fv<V> *items = reinterpret_cast<fv<V> *>(wbase);
   fv<V> *carry = items + kBatch * 32;  // rows d..S-1
   fv<V> *pre = carry;                  // rows 0..d-1
-  uint2 *ustage = reinterpret_cast<uint2 *>(carry + (a.N - 1) * 32);
+  uint4 *ustage = reinterpret_cast<uint4 *>(carry + (a.N - 1) * 32);
   uint32_t *xbuf = reinterpret_cast<uint32_t *>(ustage + kBatch);
   const int col = lane * V;
   const bool act = col < a.R;
@@ -314,8 +320,10 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     for (int l = d; l < S - 1; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
     if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
     const RowSrc<V, FT> Us(a.U_src, a.ldr, col, act);
-    fv<V> acc = fv_fill<V>(0.f);  // open node of level S-1
-    constexpr int SB = 16 / V;    // unit rows in flight per lane
+    const RowSrc<V, FT> Up(FUSE ? a.U[S - 1] : a.U_src, a.ldr, col, act);
+    const int top = FUSE ? S - 2 : S - 1;  // level whose open node the units feed
+    fv<V> acc = fv_fill<V>(0.f);           // open node of level `top`
+    constexpr int SB = (FUSE ? 8 : 16) / V;  // unit rows in flight per lane
     const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
     const uint64_t u1 = min(u0 + a.chunk, a.nunits);
     for (uint64_t base = u0; base < u1; base += kBatch) {
@@ -326,35 +334,50 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
       const uint32_t cd = in ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
       const uint32_t M = __ballot_sync(~0u, cd >= 1u);
-      ustage[lane] = make_uint2(id, __float_as_uint(v));
+      uint32_t pfid = 0u;
+      if constexpr (FUSE) {
+        // unit lane sits in level-(S-1) node first + (closes before it)
+        const uint64_t pn = (uint64_t)__shfl_sync(~0u, nodeL, S - 1) + __popc(M & lanemask_lt());
+        if (in && pn < a.nfibs[S - 1]) pfid = __ldg(a.fids[S - 1] + pn);
+      }
+      const uint32_t Mc = FUSE ? __ballot_sync(~0u, cd >= 2u) : M;  // closes of level `top`
+      ustage[lane] = make_uint4(id, __float_as_uint(v), pfid, 0u);
       __syncwarp();
       int j = 0;
       auto run = [&](auto full) {
         constexpr bool FULL = decltype(full)::value;
-  #pragma unroll
+#pragma unroll
         for (int k0 = 0; k0 < kBatch; k0 += SB) {
           if (!FULL && k0 >= cnt) break;
           fv<V> g[SB];
+          fv<V> h[FUSE ? SB : 1];
           fv<V> m[LEAF ? 1 : SB];
           float vv[LEAF ? SB : 1];
-  #pragma unroll
+#pragma unroll
           for (int q = 0; q < SB; ++q) {
             const int k = k0 + q;
             // lanes past the rank read column 0 through Us's base, so only
             // the units past the batch need the row-0 substitute
             const bool ok = FULL || k < cnt;
-            const uint2 e = ustage[k];
+            const uint4 e = ustage[k];
             g[q] = Us.load(e.x, ok);
+            if constexpr (FUSE) h[q] = Up.load(e.z, ok);
             if constexpr (LEAF) vv[q] = __uint_as_float(e.y);
             if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok && act);
           }
-  #pragma unroll
+#pragma unroll
           for (int q = 0; q < SB; ++q) {
             const int k = k0 + q;
             if (FULL || k < cnt) {
-              if constexpr (LEAF) fv_axpy(acc, vv[LEAF ? q : 0], g[q]);
-              else fv_fma(acc, m[LEAF ? 0 : q], g[q]);
-              if ((M >> k) & 1u) {
+              if constexpr (FUSE) {
+                const fv<V> x = LEAF ? fv_scale(vv[LEAF ? q : 0], g[q]) : fv_mul(m[LEAF ? 0 : q], g[q]);
+                fv_fma(acc, x, h[FUSE ? q : 0]);
+              } else if constexpr (LEAF) {
+                fv_axpy(acc, vv[LEAF ? q : 0], g[q]);
+              } else {
+                fv_fma(acc, m[LEAF ? 0 : q], g[q]);
+              }
+              if ((Mc >> k) & 1u) {
                 items[j * 32 + lane] = acc;
                 acc = fv_fill<V>(0.f);
                 ++j;
@@ -365,12 +388,16 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       };
       if (cnt == kBatch) run(std::true_type{});
       else run(std::false_type{});
-      if ((M >> (cnt - 1)) & 1u) touched &= ~(1u << (S - 1));
-      else touched |= 1u << (S - 1);
-      int n = __popc(M);
-      uint32_t icd = compact_bits(M, cd - 1u, xbuf, lane);
+      if ((Mc >> (cnt - 1)) & 1u) touched &= ~(1u << top);
+      else touched |= 1u << top;
+      if (FUSE && M != 0u) {
+        if (lane == S - 1) nodeL += (uint32_t)__popc(M);
+        part &= ~(1u << (S - 1));
+      }
+      int n = __popc(Mc);
+      uint32_t icd = compact_bits(Mc, cd - (FUSE ? 2u : 1u), xbuf, lane);
       // the level loop: items of level l (node sums that closed in this batch)
-      for (int l = S - 1; l >= d && n > 0; --l) {
+      for (int l = top; l >= d && n > 0; --l) {
         const uint32_t first = __shfl_sync(~0u, nodeL, l);
         const bool pfirst = (part >> l) & 1u;
         const uint32_t fid =
@@ -426,9 +453,9 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
         }
       }
     }
-    // chunk end: the open nodes of levels S-1 .. d add their partial sums
-    carry[(S - 1) * 32 + lane] = acc;
-    for (int l = S - 1; l >= d; --l) {
+    // chunk end: the open nodes of levels top .. d add their partial sums
+    carry[top * 32 + lane] = acc;
+    for (int l = top; l >= d; --l) {
       if (!((touched >> l) & 1u)) continue;
       const uint32_t node = __shfl_sync(~0u, nodeL, l);
       if ((uint64_t)node >= a.nfibs[l]) continue;
@@ -696,20 +723,34 @@ unsigned resident_blocks(K kernel, int threads, size_t smem) {
   return (unsigned)std::max(1, sms * std::max(1, per_sm));
 }
 
-template <int V, FactorType FT, bool LEAF>
+template <int V, FactorType FT, bool LEAF, bool FUSE>
 void launch_contract_v(const WalkArgs &a, unsigned blocks, cudaStream_t s) {
   const size_t smem = contract_smem<V>(a.N);
-  blocks = std::min(blocks, resident_blocks(k_contract<V, FT, LEAF>, 256, smem));
+  blocks = std::min(blocks, resident_blocks(k_contract<V, FT, LEAF, FUSE>, 256, smem));
   ADATM_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), s));
-  k_contract<V, FT, LEAF><<<blocks, 256, smem, s>>>(a);
+  k_contract<V, FT, LEAF, FUSE><<<blocks, 256, smem, s>>>(a);
 }
+
+// Level S-1 can be folded into the source loop when it is neither stored nor
+// the output level.
+bool fusable(const WalkArgs &a) { return a.S - 1 > a.d && a.store[a.S - 1] == nullptr; }
 
 template <FactorType FT, bool LEAF>
 void launch_contract(int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+  const bool fuse = fusable(a);
   switch (vec) {
-    case 1: launch_contract_v<1, FT, LEAF>(a, blocks, s); break;
-    case 2: launch_contract_v<2, FT, LEAF>(a, blocks, s); break;
-    case 4: launch_contract_v<4, FT, LEAF>(a, blocks, s); break;
+    case 1:
+      if (fuse) launch_contract_v<1, FT, LEAF, true>(a, blocks, s);
+      else launch_contract_v<1, FT, LEAF, false>(a, blocks, s);
+      break;
+    case 2:
+      if (fuse) launch_contract_v<2, FT, LEAF, true>(a, blocks, s);
+      else launch_contract_v<2, FT, LEAF, false>(a, blocks, s);
+      break;
+    case 4:
+      if (fuse) launch_contract_v<4, FT, LEAF, true>(a, blocks, s);
+      else launch_contract_v<4, FT, LEAF, false>(a, blocks, s);
+      break;
     default: throw BadInput("unsupported columns per lane");
   }
   ADATM_LAUNCH();
@@ -750,7 +791,10 @@ void set_walk_attributes() {
   static bool done = false;
   if (done) return;
 #define ADATM_ATTR_C(V, FT, LEAF)                                                 \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF>,                        \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, false>,                 \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                  (int)contract_smem<V>(kMaxModes)));             \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, true>,                  \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)contract_smem<V>(kMaxModes)));
 #define ADATM_ATTR_S(W, FT, LEAF)                                                 \
