@@ -1,5 +1,8 @@
 // engine.cu -- tensor + plan + trees + memo rows + factors + CP-ALS sweep.
 #include <algorithm>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
 #include <thread>
 #include <cmath>
 #include <cstring>
@@ -9,23 +12,76 @@
 namespace adatm {
 
 namespace {
-// Rows [0, rows) of a host conversion split over a few threads when large.
+// Host workers for the factor conversions at the C-ABI boundary, started
+// once: starting threads on every call costs more than the conversion. A
+// call splits rows [0, rows) into parts, runs part 0 itself and waits for the
+// rest; calls are serialised.
+class HostPool {
+ public:
+  static HostPool &instance() {
+    static HostPool *p = new HostPool();  // never destroyed: its workers are detached
+    return *p;
+  }
+  void run(uint64_t rows, unsigned parts, const std::function<void(uint64_t, uint64_t)> &f) {
+    parts = std::min<unsigned>(parts, nworkers_ + 1);
+    if (parts <= 1 || rows < 2) {
+      f(0, rows);
+      return;
+    }
+    std::lock_guard<std::mutex> one(call_mu_);
+    const uint64_t step = (rows + parts - 1) / parts;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &f;
+      rows_ = rows;
+      step_ = step;
+      left_ = parts - 1;
+      next_ = 1;
+      parts_ = parts;
+    }
+    cv_.notify_all();
+    f(0, std::min(rows, step));
+    std::unique_lock<std::mutex> lk(mu_);
+    done_.wait(lk, [&] { return left_ == 0; });
+    parts_ = 0;
+    next_ = 0;
+    fn_ = nullptr;
+  }
+
+ private:
+  HostPool() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    nworkers_ = std::min(7u, hw > 1 ? hw - 1 : 0u);
+    for (unsigned t = 0; t < nworkers_; ++t) std::thread([this] { loop(); }).detach();
+  }
+  void loop() {
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+      cv_.wait(lk, [&] { return next_ < parts_; });
+      while (next_ < parts_) {
+        const unsigned p = next_++;
+        const auto *fn = fn_;
+        const uint64_t a = p * step_, b = std::min(rows_, a + step_);
+        lk.unlock();
+        if (a < b) (*fn)(a, b);
+        lk.lock();
+        if (--left_ == 0) done_.notify_one();
+      }
+    }
+  }
+  unsigned nworkers_ = 0;
+  std::mutex call_mu_, mu_;
+  std::condition_variable cv_, done_;
+  const std::function<void(uint64_t, uint64_t)> *fn_ = nullptr;
+  uint64_t rows_ = 0, step_ = 0;
+  unsigned parts_ = 0, next_ = 0, left_ = 0;
+};
+
+// Rows [0, rows) of a host conversion, split over the pool when large.
 template <typename F>
 void host_rows(uint64_t rows, uint64_t row_elems, F &&f) {
-  const uint64_t work = rows * row_elems;
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned nt = (unsigned)std::min<uint64_t>({(uint64_t)std::min(hw, 8u), work / 65536 + 1, rows});
-  if (nt <= 1) {
-    f(0, rows);
-    return;
-  }
-  std::vector<std::thread> ts;
-  const uint64_t step = (rows + nt - 1) / nt;
-  for (unsigned t = 0; t < nt; ++t) {
-    const uint64_t a = t * step, b = std::min(rows, a + step);
-    if (a < b) ts.emplace_back([&f, a, b] { f(a, b); });
-  }
-  for (auto &th : ts) th.join();
+  const unsigned parts = (unsigned)std::min<uint64_t>(8, rows * row_elems / 32768 + 1);
+  HostPool::instance().run(rows, parts, std::function<void(uint64_t, uint64_t)>(f));
 }
 
 int depth_of(const DevCsf &c, int mode) {

@@ -578,27 +578,38 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
       const int ke = min(deep, cnt - 1);
       float4 Q = make_float4(1.f, 1.f, 1.f, 1.f);
       if (d >= 2 && act) Q = *reinterpret_cast<const float4 *>(preq + (d - 2) * a.ldr + col);
-      for (int k0 = k; k0 <= ke; k0 += UPS) {
-        const int unit = k0 + slot;
-        const bool ok = unit <= ke && act;
-        const uint2 e = ustage[unit & 31];
-        float4 p = make_float4(1.f, 1.f, 1.f, 1.f);
-        if (d >= 1) {
-          const uint32_t f = pstage[__popc(M & ((1u << (unit & 31)) - 1u))];
-          const float4 r = ld_factor4<FT>(a.U[d - 1], f, a.ldr, col, ok);
-          p = make_float4(Q.x * r.x, Q.y * r.y, Q.z * r.z, Q.w * r.w);
+      // four steps' row loads are issued before any of their products
+      constexpr int ST = 4;
+      for (int k0 = k; k0 <= ke; k0 += ST * UPS) {
+        float4 r[ST];
+        fv<4> m[LEAF ? 1 : ST];
+#pragma unroll
+        for (int t = 0; t < ST; ++t) {
+          const int unit = k0 + t * UPS + slot;
+          const bool ok = unit <= ke && act;
+          r[t] = make_float4(1.f, 1.f, 1.f, 1.f);
+          if (d >= 1) r[t] = ld_factor4<FT>(a.U[d - 1], pstage[__popc(M & ((1u << (unit & 31)) - 1u))],
+                                            a.ldr, col, ok);
+          if constexpr (!LEAF) m[t] = ld_rows<4>(a.src_rows, base + (unit & 31), a.ldr, col, ok);
         }
-        float4 x;
-        if constexpr (LEAF) {
-          const float s = __uint_as_float(e.y);
-          x = make_float4(s * p.x, s * p.y, s * p.z, s * p.w);
-        } else {
-          const fv<4> m = ld_rows<4>(a.src_rows, base + (unit & 31), a.ldr, col, ok);
-          x = make_float4(m.x[0] * p.x, m.x[1] * p.y, m.x[2] * p.z, m.x[3] * p.w);
-        }
-        if (ok) {
-          if (stage) sts4(xs + (unit & 31) * a.ldr + col, x);
-          else atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)e.x * a.ldr + col), x);
+#pragma unroll
+        for (int t = 0; t < ST; ++t) {
+          const int unit = k0 + t * UPS + slot;
+          const bool ok = unit <= ke && act;
+          const uint2 e = ustage[unit & 31];
+          const float4 p = d >= 1 ? make_float4(Q.x * r[t].x, Q.y * r[t].y, Q.z * r[t].z, Q.w * r[t].w)
+                                  : r[t];
+          float4 x;
+          if constexpr (LEAF) {
+            const float sv = __uint_as_float(e.y);
+            x = make_float4(sv * p.x, sv * p.y, sv * p.z, sv * p.w);
+          } else {
+            x = make_float4(m[t].x[0] * p.x, m[t].x[1] * p.y, m[t].x[2] * p.z, m[t].x[3] * p.w);
+          }
+          if (ok) {
+            if (stage) sts4(xs + (unit & 31) * a.ldr + col, x);
+            else atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)e.x * a.ldr + col), x);
+          }
         }
       }
       if (deep == ke) {
