@@ -135,14 +135,17 @@ Engine::Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<De
   ADATM_CUDA(cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking));
   ADATM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
   ADATM_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
+  ADATM_CUDA(cudaEventCreateWithFlags(&staged_, cudaEventDisableTiming));
   build_walks();
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
 Engine::~Engine() {
+  if (staged_pending_) cudaEventSynchronize(staged_);
   drop_graph();
   if (join_) cudaEventDestroy(join_);
   if (fork_) cudaEventDestroy(fork_);
+  if (staged_) cudaEventDestroy(staged_);
   if (side_) cudaStreamDestroy(side_);
   if (staging_) cudaFreeHost(staging_);
 }
@@ -161,6 +164,15 @@ void Engine::set_chunks(uint32_t chunk_leaf, uint32_t chunk_rows) {
   opt_.chunk_rows = chunk_rows;
   build_walks();
   ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::set_resident_grid(bool on) {
+  drop_graph();
+  opt_.resident_grid = on;
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    walk_[m]->resident = on;
+    direct_[m]->resident = on;
+  }
 }
 
 float Engine::time_sweeps(int count) {
@@ -203,6 +215,9 @@ BatchSweep::BatchSweep(std::vector<Engine *> engines, cudaStream_t stream)
   if (e_.empty()) throw BadInput("an empty batch");
   for (Engine *e : e_)
     if (!e) throw BadInput("a null engine in the batch");
+  // the branches' walks run side by side: one chunk per warp, so their
+  // blocks interleave instead of each walk holding every SM in turn
+  for (Engine *e : e_) e->set_resident_grid(false);
   ADATM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
   join_.resize(e_.size(), nullptr);
   for (auto &ev : join_) ADATM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -266,6 +281,11 @@ int BatchSweep::kernels_per_sweep() const {
 }
 
 float *Engine::staging(size_t n) {
+  // the host may write the rows only once the copies that read them are done
+  if (staged_pending_) {
+    ADATM_CUDA(cudaEventSynchronize(staged_));
+    staged_pending_ = false;
+  }
   if (n > staging_n_) {
     if (staging_) cudaFreeHost(staging_);
     staging_ = nullptr;
@@ -304,6 +324,7 @@ void Engine::build_walks() {
     direct->src = N - 1;
     direct->out = d;
     direct->chunk = opt_.chunk_leaf;
+    direct->resident = opt_.resident_grid;
     walk_prepare(*direct, stream_);
     auto w = std::make_unique<TreeWalk>();
     w->csf = &c;
@@ -312,6 +333,7 @@ void Engine::build_walks() {
     w->src = N - 1;
     w->out = d;
     w->chunk = opt_.chunk_leaf;
+    w->resident = opt_.resident_grid;
     if (tag == 0 && gp.n_imten > 0) {
       // memo root: store level begin_imten-1-deg into memo tree deg
       for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
@@ -421,7 +443,9 @@ void Engine::set_factors(const double *const *host) {
     if (Ab_[m].get()) to_bf16(A_[m].get(), Ab_[m].get(), I, ldr_, stream_);
     off += (size_t)I * ldr_;
   }
-  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  // the copies run on; the staging rows are not reused before they end
+  ADATM_CUDA(cudaEventRecord(staged_, stream_));
+  staged_pending_ = true;
 }
 
 void Engine::get_factors(double *const *host) {
@@ -448,23 +472,28 @@ void Engine::get_normalized(double *const *host, double *lambda) {
   const int N = coo_->nmodes;
   size_t total = 0;
   for (int m = 0; m < N; ++m) total += (size_t)coo_->dims[m] * ldr_;
-  float *buf = staging(total);
-  std::vector<double> diag((size_t)N * R_ * R_);
+  // factor rows, then the Grams and lambda (FP64, 8-byte aligned: total is
+  // a multiple of 4 floats), all into the pinned staging rows, one sync
+  const size_t extra = 2 * ((size_t)N * R_ * R_ + R_);
+  float *buf = staging(total + extra);
+  double *diag = reinterpret_cast<double *>(buf + total);
+  double *lam = diag + (size_t)N * R_ * R_;
   size_t off = 0;
   for (int m = 0; m < N; ++m) {
     ADATM_CUDA(cudaMemcpyAsync(buf + off, A_[m].get(), (size_t)coo_->dims[m] * ldr_ * sizeof(float),
                                cudaMemcpyDeviceToHost, stream_));
-    ADATM_CUDA(cudaMemcpyAsync(diag.data() + (size_t)m * R_ * R_, G_[m].get(),
-                               R_ * R_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    ADATM_CUDA(cudaMemcpyAsync(diag + (size_t)m * R_ * R_, G_[m].get(), R_ * R_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_));
     off += (size_t)coo_->dims[m] * ldr_;
   }
-  ADATM_CUDA(cudaMemcpyAsync(lambda, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost,
+  ADATM_CUDA(cudaMemcpyAsync(lam, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost,
                              stream_));
   ADATM_CUDA(cudaStreamSynchronize(stream_));
+  std::memcpy(lambda, lam, R_ * sizeof(double));
   std::vector<double> inv(R_);
   off = 0;
   for (int m = 0; m < N; ++m) {
-    const double *G = diag.data() + (size_t)m * R_ * R_;
+    const double *G = diag + (size_t)m * R_ * R_;
     for (uint64_t r = 0; r < R_; ++r) {
       const double nrm = std::sqrt(std::max(G[r * R_ + r], 0.0));
       inv[r] = nrm > 0 ? 1.0 / nrm : 0.0;
@@ -498,7 +527,6 @@ void Engine::als_begin() {
   }
   ADATM_CUDA(cudaMemsetAsync(w_.iter.get(), 0, sizeof(int), stream_));
   ADATM_CUDA(cudaMemsetAsync(w_.fit_trace.get(), 0, w_.max_trace * sizeof(double), stream_));
-  ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
 void Engine::sweep_eager() {

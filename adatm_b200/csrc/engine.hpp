@@ -16,6 +16,10 @@ struct EngineOptions {
   uint32_t chunk_leaf = 256;  // source units per chunk (one warp), nonzero sources
   uint32_t chunk_rows = 128;  // source units per chunk (one warp), memo-row sources
   int max_iters = 1024;       // capacity of the device fit trace
+  // contraction walks as a resident grid whose warps claim chunks (fastest
+  // for one tensor on the device); off, one chunk per warp, so the blocks of
+  // walks running side by side on other streams interleave
+  bool resident_grid = true;
 };
 
 class Engine {
@@ -85,6 +89,9 @@ class Engine {
   // Rebuild the walk schedules with other chunk sizes (drops a captured
   // graph). Factors, Grams and memo rows stay as they are.
   void set_chunks(uint32_t chunk_leaf, uint32_t chunk_rows);
+  // Contraction grid shape (EngineOptions::resident_grid); drops a captured
+  // sweep.
+  void set_resident_grid(bool on);
   uint32_t chunk_leaf() const { return opt_.chunk_leaf; }
   uint32_t chunk_rows() const { return opt_.chunk_rows; }
   // Time `count` graph-replayed sweeps (CUDA events, ms total).
@@ -124,6 +131,8 @@ class Engine {
   // MTTKRP (it reads only the other modes' Grams); fork / join events.
   cudaStream_t side_ = nullptr;
   cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  cudaEvent_t staged_ = nullptr;  // after the last copy that reads the staging rows
+  bool staged_pending_ = false;
 };
 
 // Many independent tensors swept together: one CUDA graph holds one ALS

@@ -308,11 +308,12 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
   const bool act = col < a.R;
   const int S = a.S, d = a.d;
   // a resident grid: each warp claims chunks from a counter, the next one
-  // while it walks the current one
-  uint32_t claim = lane == 0 ? atomicAdd(a.counter, 1u) : 0u;
-  uint32_t chunk_id = __shfl_sync(~0u, claim, 0);
+  // while it walks the current one; without a counter, one chunk per warp
+  const bool claims = a.counter != nullptr;
+  uint32_t claim = claims && lane == 0 ? atomicAdd(a.counter, 1u) : 0u;
+  uint32_t chunk_id = claims ? __shfl_sync(~0u, claim, 0) : blockIdx.x * kWarps + warp;
   while (chunk_id < a.nchunks) {
-    claim = lane == 0 ? atomicAdd(a.counter, 1u) : 0u;
+    if (claims && lane == 0) claim = atomicAdd(a.counter, 1u);
     const uint32_t *sc = a.sched + (size_t)chunk_id * (S + 1);
     uint32_t nodeL = lane < S ? sc[lane] : 0u;
     uint32_t part = sc[S];
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       }
     }
     __syncwarp();
-    chunk_id = __shfl_sync(~0u, claim, 0);
+    chunk_id = claims ? __shfl_sync(~0u, claim, 0) : a.nchunks;
   }
 }
 
@@ -735,11 +736,17 @@ unsigned resident_blocks(K kernel, int threads, size_t smem) {
 }
 
 template <int V, FactorType FT, bool LEAF, bool FUSE>
-void launch_contract_v(const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+void launch_contract_v(const WalkArgs &a, unsigned blocks, bool resident, cudaStream_t s) {
   const size_t smem = contract_smem<V>(a.N);
-  blocks = std::min(blocks, resident_blocks(k_contract<V, FT, LEAF, FUSE>, 256, smem));
-  ADATM_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), s));
-  k_contract<V, FT, LEAF, FUSE><<<blocks, 256, smem, s>>>(a);
+  if (resident) {
+    blocks = std::min(blocks, resident_blocks(k_contract<V, FT, LEAF, FUSE>, 256, smem));
+    ADATM_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), s));
+    k_contract<V, FT, LEAF, FUSE><<<blocks, 256, smem, s>>>(a);
+  } else {
+    WalkArgs b = a;
+    b.counter = nullptr;  // one chunk per warp: blocks cover every chunk
+    k_contract<V, FT, LEAF, FUSE><<<blocks, 256, smem, s>>>(b);
+  }
 }
 
 // Level S-1 can be folded into the source loop when it is neither stored nor
@@ -747,20 +754,20 @@ void launch_contract_v(const WalkArgs &a, unsigned blocks, cudaStream_t s) {
 bool fusable(const WalkArgs &a) { return a.S - 1 > a.d && a.store[a.S - 1] == nullptr; }
 
 template <FactorType FT, bool LEAF>
-void launch_contract(int vec, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+void launch_contract(int vec, const WalkArgs &a, unsigned blocks, bool resident, cudaStream_t s) {
   const bool fuse = fusable(a);
   switch (vec) {
     case 1:
-      if (fuse) launch_contract_v<1, FT, LEAF, true>(a, blocks, s);
-      else launch_contract_v<1, FT, LEAF, false>(a, blocks, s);
+      if (fuse) launch_contract_v<1, FT, LEAF, true>(a, blocks, resident, s);
+      else launch_contract_v<1, FT, LEAF, false>(a, blocks, resident, s);
       break;
     case 2:
-      if (fuse) launch_contract_v<2, FT, LEAF, true>(a, blocks, s);
-      else launch_contract_v<2, FT, LEAF, false>(a, blocks, s);
+      if (fuse) launch_contract_v<2, FT, LEAF, true>(a, blocks, resident, s);
+      else launch_contract_v<2, FT, LEAF, false>(a, blocks, resident, s);
       break;
     case 4:
-      if (fuse) launch_contract_v<4, FT, LEAF, true>(a, blocks, s);
-      else launch_contract_v<4, FT, LEAF, false>(a, blocks, s);
+      if (fuse) launch_contract_v<4, FT, LEAF, true>(a, blocks, resident, s);
+      else launch_contract_v<4, FT, LEAF, false>(a, blocks, resident, s);
       break;
     default: throw BadInput("unsupported columns per lane");
   }
@@ -858,11 +865,11 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
   if (w.src > w.out) {
     const int vec = vec_for_rank(w.R);
     if (ft == FactorType::F32) {
-      if (leaf) launch_contract<FactorType::F32, true>(vec, a, blocks, s);
-      else launch_contract<FactorType::F32, false>(vec, a, blocks, s);
+      if (leaf) launch_contract<FactorType::F32, true>(vec, a, blocks, w.resident, s);
+      else launch_contract<FactorType::F32, false>(vec, a, blocks, w.resident, s);
     } else {
-      if (leaf) launch_contract<FactorType::BF16, true>(vec, a, blocks, s);
-      else launch_contract<FactorType::BF16, false>(vec, a, blocks, s);
+      if (leaf) launch_contract<FactorType::BF16, true>(vec, a, blocks, w.resident, s);
+      else launch_contract<FactorType::BF16, false>(vec, a, blocks, w.resident, s);
     }
   } else {
     const int lanes = lanes_for_rank(w.R);

@@ -46,7 +46,9 @@ struct TreeWalk {
   const DevCsf *csf = nullptr;
   const float *src_rows = nullptr;           // memo rows of level S (S < N-1)
   float *store[kMaxModes] = {nullptr};       // memo rows written, per level
-  DevBuf<uint32_t> sched;                    // nchunks x (S + 1)
+  DevBuf<uint32_t> sched;                    // nchunks x (S + 1), then the chunk counter
+  bool resident = true;                      // contraction grid: resident blocks that claim
+                                             // chunks (else one chunk per warp)
   bool has_store() const {
     for (int l = 0; l < kMaxModes; ++l)
       if (store[l]) return true;
