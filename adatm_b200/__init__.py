@@ -746,6 +746,12 @@ class Engine:
                "adatm_engine_autotune")
         return best.value
 
+    def set_resident_grid(self, on):
+        """Contraction walks as a resident grid claiming chunks (True, the
+        default) or one chunk per warp (False, as in a batch)."""
+        _check(lib().adatm_engine_set_resident_grid(self._h, int(bool(on))),
+               "adatm_engine_set_resident_grid")
+
 
 class BatchSweep:
     """One ALS iteration of every engine in one CUDA graph; the engines must

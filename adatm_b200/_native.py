@@ -150,6 +150,7 @@ _SIGS = [
     ("adatm_engine_mttkrp_bytes", C.c_int, [C.c_void_p, u64, P_f64]),
     ("adatm_engine_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                         C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    ("adatm_engine_set_resident_grid", C.c_int, [C.c_void_p, C.c_int]),
     ("adatm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("adatm_batch_begin", C.c_int, [C.c_void_p]),
     ("adatm_batch_time_sweeps", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),

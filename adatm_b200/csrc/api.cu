@@ -1157,6 +1157,14 @@ int adatm_engine_autotune(adatm_engine *e, const uint32_t *chunk_leaf, const uin
   });
 }
 
+int adatm_engine_set_resident_grid(adatm_engine *e, int on) {
+  return guarded([&] {
+    if (!e) throw BadInput("adatm_engine_set_resident_grid: null engine");
+    e->eng->set_resident_grid(on != 0);
+    e->graph = false;
+  });
+}
+
 int adatm_batch_create(adatm_engine *const *engines, int n, adatm_batch **out) {
   return guarded([&] {
     if (n < 1 || !engines || !out) throw BadInput("adatm_batch_create: no engines");

@@ -263,6 +263,13 @@ int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
 int adatm_engine_autotune(adatm_engine *e, const uint32_t *chunk_leaf, const uint32_t *chunk_rows,
                           int n, int sweeps, int *best);
 
+/* Contraction walks as a resident grid whose warps claim chunks from a
+ * counter (on: the default, fastest for one tensor on the device) or one
+ * chunk per warp (off: what a batch uses, so the blocks of walks on
+ * concurrent streams interleave). Results agree up to FP32 summation order.
+ * Drops a captured sweep. No reference counterpart (a launch-shape control). */
+int adatm_engine_set_resident_grid(adatm_engine *e, int on);
+
 /* One ALS iteration of every engine in one CUDA graph (each engine on its
  * own branch). The engines must outlive the batch. */
 typedef struct adatm_batch adatm_batch;

@@ -60,3 +60,27 @@ def test_autotune_keeps_results(gpu):
         m0 = e0.mttkrp(m)
         m1 = e1.mttkrp(m)
         assert np.max(np.abs(m0 - m1)) <= 1e-5 * np.max(np.abs(m0))
+
+
+@pytest.mark.parametrize("R", [8, 32, 64])
+def test_resident_and_per_warp_grids_agree(gpu, R):
+    """The contraction grid shapes (resident blocks claiming chunks from a
+    counter, and one chunk per warp as batches use) give the same MTTKRP
+    sequence up to FP32 summation order, on memo-root, folded and plain
+    walks."""
+    import oracle as O
+    A = gpu
+    for k, (dims, nnz, alpha) in enumerate(SHAPES):
+        t = A.Tensor.generate(dims, nnz, alpha=alpha, seed=300 + k)
+        plan, _, _ = A.plan_analytic(t, R)
+        mats = O.init_factors(list(t.info()[2]), R, 7)
+        e0 = A.Engine(t, R, plan)
+        e1 = A.Engine(t, R, plan)
+        e1.set_resident_grid(False)
+        e0.set_factors(mats)
+        e1.set_factors(mats)
+        for m in range(len(dims)):
+            a, b = e0.mttkrp(m), e1.mttkrp(m)
+            assert np.max(np.abs(a - b)) <= 2e-5 * max(1e-30, np.max(np.abs(a))), (k, m)
+        e0.free()
+        e1.free()
