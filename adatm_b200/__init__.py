@@ -729,6 +729,12 @@ class Engine:
         _check(lib().adatm_engine_mttkrp_bytes(self._h, mode, C.byref(b)), "mttkrp_bytes")
         return b.value
 
+    def hot_rows(self, mode):
+        """Output rows the mode's walk sums per block in shared memory."""
+        n = C.c_int(0)
+        _check(lib().adatm_engine_hot_rows(self._h, mode, C.byref(n)), "hot_rows")
+        return n.value
+
     def launch_counts(self, mode=0):
         a = C.c_int(0)
         b = C.c_int(0)

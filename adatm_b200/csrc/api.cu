@@ -1145,6 +1145,14 @@ int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes) {
   });
 }
 
+int adatm_engine_hot_rows(adatm_engine *e, uint64_t mode, int *nhot) {
+  return guarded([&] {
+    if (!e || !nhot) throw BadInput("adatm_engine_hot_rows: null argument");
+    if (mode >= (uint64_t)e->eng->nmodes()) throw BadInput("mode out of range");
+    *nhot = e->eng->walk((int)mode).nhot;
+  });
+}
+
 int adatm_engine_autotune(adatm_engine *e, const uint32_t *chunk_leaf, const uint32_t *chunk_rows,
                           int n, int sweeps, int *best) {
   return guarded([&] {

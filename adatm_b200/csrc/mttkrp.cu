@@ -1,6 +1,7 @@
 // mttkrp.cu -- tree-walk MTTKRP kernels (see mttkrp.cuh for the scheme).
 #include <algorithm>
 #include <type_traits>
+#include <vector>
 
 #include "mttkrp.cuh"
 
@@ -25,7 +26,13 @@ struct WalkArgs {
   float *out;
   const uint32_t *sched;
   uint32_t *counter;           // chunks claimed so far (zeroed before each launch)
+  const uint8_t *hot_slot;     // scatter: slot of an output row summed per block, 0xFF = none
+  const uint32_t *hot_rows;    // scatter: output row of each slot
+  int nhot;
 };
+
+constexpr int kHotRows = 32;     // output rows summed per block, at most
+constexpr uint32_t kHotMin = 32768;  // units that must hit a row to make it one
 
 // ---------------------------------------------------------------------------
 // Warp-uniform tree walk.
@@ -527,13 +534,11 @@ __device__ __noinline__ void scatter_prefix(const WalkArgs &a, float *preq, uint
   }
 }
 
-template <int W, FactorType FT, bool LEAF>
-__global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ WalkArgs a) {
+template <int W, FactorType FT, bool LEAF, bool HOT>
+__global__ void __launch_bounds__(256, HOT ? 3 : 1) k_scatter(const __grid_constant__ WalkArgs a) {
   constexpr int UPS = 32 / W;  // units per step
   extern __shared__ __align__(16) unsigned char walk_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t chunk_id = blockIdx.x * kWarps + warp;
-  if (chunk_id >= a.nchunks) return;
   unsigned char *wbase = walk_raw + (size_t)warp * scatter_warp_bytes(a.ldr);
   float *preq = reinterpret_cast<float *>(wbase);  // kMaxModes x ldr columns
   uint2 *ustage = reinterpret_cast<uint2 *>(preq + kMaxModes * a.ldr);
@@ -545,110 +550,151 @@ __global__ void __launch_bounds__(256, 1) k_scatter(const __grid_constant__ Walk
   const int col = 4 * (lane % W);
   const bool act = col < a.R;
   const int d = a.S;
-  const uint32_t *sc = a.sched + (size_t)chunk_id * (d + 1);
-  uint32_t nodeL = lane < d ? sc[lane] : 0u;
-  if (d >= 2) scatter_prefix<FT>(a, preq, nodeL, 0, d - 1, lane);
-  __syncwarp();
-  const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
-  const uint64_t u1 = min(u0 + a.chunk, a.nunits);
-  for (uint64_t base = u0; base < u1; base += kBatch) {
-    const int cnt = (int)min((uint64_t)kBatch, u1 - base);
-    const bool in = lane < cnt;
-    const uint32_t id = in ? __ldg(a.src_ids + base + lane) : 0u;
-    float v = 0.f;
-    if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
-    const uint32_t cd = (in && d >= 1) ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
-    const uint32_t M = __ballot_sync(~0u, cd >= 1u);
-    const uint32_t M2 = __ballot_sync(~0u, cd >= 2u);
-    // factor-row ids of the parents (level d-1) of this batch's units
-    const uint32_t nodeP = d >= 1 ? __shfl_sync(~0u, nodeL, d - 1) : 0u;
-    uint32_t pf = 0;
-    if (d >= 1 && (uint64_t)nodeP + lane < a.nfibs[d - 1]) pf = __ldg(a.fids[d - 1] + nodeP + lane);
-    ustage[lane] = make_uint2(id, __float_as_uint(v));
-    pstage[lane] = pf;
-    // units of this batch that repeat an output row
-    const uint32_t grp = __match_any_sync(~0u, in ? id : 0xFFFFFFFFu);
-    const bool lead = in && (grp & lanemask_lt()) == 0;
-    const bool stage = __ballot_sync(~0u, in && !lead) != 0u;
-    gstage[lane] = grp;
-    __syncwarp();
-    int k = 0;
-    while (k < cnt) {
-      const uint32_t rest = M2 & (~0u << k);
-      const int deep = rest ? __ffs(rest) - 1 : 32;
-      const int ke = min(deep, cnt - 1);
-      float4 Q = make_float4(1.f, 1.f, 1.f, 1.f);
-      if (d >= 2 && act) Q = *reinterpret_cast<const float4 *>(preq + (d - 2) * a.ldr + col);
-      // four steps' row loads are issued before any of their products
-      constexpr int ST = 4;
-      for (int k0 = k; k0 <= ke; k0 += ST * UPS) {
-        float4 r[ST];
-        fv<4> m[LEAF ? 1 : ST];
-#pragma unroll
-        for (int t = 0; t < ST; ++t) {
-          const int unit = k0 + t * UPS + slot;
-          const bool ok = unit <= ke && act;
-          r[t] = make_float4(1.f, 1.f, 1.f, 1.f);
-          if (d >= 1) r[t] = ld_factor4<FT>(a.U[d - 1], pstage[__popc(M & ((1u << (unit & 31)) - 1u))],
-                                            a.ldr, col, ok);
-          if constexpr (!LEAF) m[t] = ld_rows<4>(a.src_rows, base + (unit & 31), a.ldr, col, ok);
-        }
-#pragma unroll
-        for (int t = 0; t < ST; ++t) {
-          const int unit = k0 + t * UPS + slot;
-          const bool ok = unit <= ke && act;
-          const uint2 e = ustage[unit & 31];
-          const float4 p = d >= 1 ? make_float4(Q.x * r[t].x, Q.y * r[t].y, Q.z * r[t].z, Q.w * r[t].w)
-                                  : r[t];
-          float4 x;
-          if constexpr (LEAF) {
-            const float sv = __uint_as_float(e.y);
-            x = make_float4(sv * p.x, sv * p.y, sv * p.z, sv * p.w);
-          } else {
-            x = make_float4(m[t].x[0] * p.x, m[t].x[1] * p.y, m[t].x[2] * p.z, m[t].x[3] * p.w);
-          }
-          if (ok) {
-            if (stage) sts4(xs + (unit & 31) * a.ldr + col, x);
-            else atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)e.x * a.ldr + col), x);
-          }
-        }
+  // hot output rows: summed by the block in shared memory, added to the
+  // output once at the end (their atomics would otherwise queue on a few L2
+  // lines); the grid is then resident and warps stride over the chunks
+  float *hacc = HOT ? reinterpret_cast<float *>(walk_raw + kWarps * scatter_warp_bytes(a.ldr)) : nullptr;
+  if constexpr (HOT) {
+    for (int i = threadIdx.x; i < a.nhot * a.ldr; i += blockDim.x) hacc[i] = 0.f;
+    __syncthreads();
+  }
+  auto emit = [&](uint32_t row, const float4 &x) {
+    if constexpr (HOT) {
+      const uint32_t sl = __ldg(a.hot_slot + row);
+      if (sl != 0xFFu) {
+        float *h = hacc + sl * a.ldr + col;
+        atomicAdd(h, x.x);
+        atomicAdd(h + 1, x.y);
+        atomicAdd(h + 2, x.z);
+        atomicAdd(h + 3, x.w);
+        return;
       }
-      if (deep == ke) {
-        // unit ke closes levels d-1 .. d-c (c >= 2): the levels above its
-        // parent move on and Q is recomputed
-        const int c = (int)__shfl_sync(~0u, cd, ke);
-        if (lane >= d - c && lane < d - 1) nodeL += 1;
-        if ((uint64_t)__shfl_sync(~0u, nodeL, d - c) < a.nfibs[d - c])
-          scatter_prefix<FT>(a, preq, nodeL, d - c, d - 1, lane);
+    }
+    atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)row * a.ldr + col), x);
+  };
+  // without hot rows the grid covers every chunk: one chunk per warp
+  for (uint32_t chunk_id = blockIdx.x * kWarps + warp; chunk_id < a.nchunks;
+       chunk_id = HOT ? chunk_id + gridDim.x * kWarps : a.nchunks) {
+    const uint32_t *sc = a.sched + (size_t)chunk_id * (d + 1);
+    uint32_t nodeL = lane < d ? sc[lane] : 0u;
+    if (d >= 2) scatter_prefix<FT>(a, preq, nodeL, 0, d - 1, lane);
+    __syncwarp();
+    const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
+    const uint64_t u1 = min(u0 + a.chunk, a.nunits);
+    for (uint64_t base = u0; base < u1; base += kBatch) {
+      const int cnt = (int)min((uint64_t)kBatch, u1 - base);
+      const bool in = lane < cnt;
+      const uint32_t id = in ? __ldg(a.src_ids + base + lane) : 0u;
+      float v = 0.f;
+      if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
+      const uint32_t cd = (in && d >= 1) ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
+      const uint32_t M = __ballot_sync(~0u, cd >= 1u);
+      const uint32_t M2 = __ballot_sync(~0u, cd >= 2u);
+      // factor-row ids of the parents (level d-1) of this batch's units
+      const uint32_t nodeP = d >= 1 ? __shfl_sync(~0u, nodeL, d - 1) : 0u;
+      uint32_t pf = 0;
+      if (d >= 1 && (uint64_t)nodeP + lane < a.nfibs[d - 1]) pf = __ldg(a.fids[d - 1] + nodeP + lane);
+      ustage[lane] = make_uint2(id, __float_as_uint(v));
+      pstage[lane] = pf;
+      // units of this batch that repeat an output row
+      const uint32_t grp = __match_any_sync(~0u, in ? id : 0xFFFFFFFFu);
+      const bool lead = in && (grp & lanemask_lt()) == 0;
+      const bool stage = __ballot_sync(~0u, in && !lead) != 0u;
+      gstage[lane] = grp;
+      __syncwarp();
+      int k = 0;
+      while (k < cnt) {
+        const uint32_t rest = M2 & (~0u << k);
+        const int deep = rest ? __ffs(rest) - 1 : 32;
+        const int ke = min(deep, cnt - 1);
+        float4 Q = make_float4(1.f, 1.f, 1.f, 1.f);
+        if (d >= 2 && act) Q = *reinterpret_cast<const float4 *>(preq + (d - 2) * a.ldr + col);
+        // four steps' row loads are issued before any of their products
+        constexpr int ST = 4;
+        for (int k0 = k; k0 <= ke; k0 += ST * UPS) {
+          float4 r[ST];
+          fv<4> m[LEAF ? 1 : ST];
+#pragma unroll
+          for (int t = 0; t < ST; ++t) {
+            const int unit = k0 + t * UPS + slot;
+            const bool ok = unit <= ke && act;
+            r[t] = make_float4(1.f, 1.f, 1.f, 1.f);
+            if (d >= 1) r[t] = ld_factor4<FT>(a.U[d - 1], pstage[__popc(M & ((1u << (unit & 31)) - 1u))],
+                                              a.ldr, col, ok);
+            if constexpr (!LEAF) m[t] = ld_rows<4>(a.src_rows, base + (unit & 31), a.ldr, col, ok);
+          }
+#pragma unroll
+          for (int t = 0; t < ST; ++t) {
+            const int unit = k0 + t * UPS + slot;
+            const bool ok = unit <= ke && act;
+            const uint2 e = ustage[unit & 31];
+            const float4 p = d >= 1 ? make_float4(Q.x * r[t].x, Q.y * r[t].y, Q.z * r[t].z, Q.w * r[t].w)
+                                    : r[t];
+            float4 x;
+            if constexpr (LEAF) {
+              const float sv = __uint_as_float(e.y);
+              x = make_float4(sv * p.x, sv * p.y, sv * p.z, sv * p.w);
+            } else {
+              x = make_float4(m[t].x[0] * p.x, m[t].x[1] * p.y, m[t].x[2] * p.z, m[t].x[3] * p.w);
+            }
+            if (ok) {
+              if (stage) sts4(xs + (unit & 31) * a.ldr + col, x);
+              else emit(e.x, x);
+            }
+          }
+        }
+        if (deep == ke) {
+          // unit ke closes levels d-1 .. d-c (c >= 2): the levels above its
+          // parent move on and Q is recomputed
+          const int c = (int)__shfl_sync(~0u, cd, ke);
+          if (lane >= d - c && lane < d - 1) nodeL += 1;
+          if ((uint64_t)__shfl_sync(~0u, nodeL, d - c) < a.nfibs[d - c])
+            scatter_prefix<FT>(a, preq, nodeL, d - c, d - 1, lane);
+          __syncwarp();
+        }
+        k = ke + 1;
+      }
+      if (stage) {
+        // one atomic per distinct output row: the leading unit sums its group
         __syncwarp();
-      }
-      k = ke + 1;
-    }
-    if (stage) {
-      // one atomic per distinct output row: the leading unit sums its group
-      __syncwarp();
-      const uint32_t L = __ballot_sync(~0u, lead);
-      if (lead) lstage[__popc(L & lanemask_lt())] = (uint32_t)lane;
-      __syncwarp();
-      const int nl = __popc(L);
-      for (int i0 = 0; i0 < nl; i0 += UPS) {
-        const int i = i0 + slot;
-        if (i < nl && act) {
-          const uint32_t u = lstage[i];
-          uint32_t members = gstage[u];
-          float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-          while (members) {
-            const int m = __ffs(members) - 1;
-            members &= members - 1u;
-            const float4 x = lds4(xs + m * a.ldr + col);
-            sum = make_float4(sum.x + x.x, sum.y + x.y, sum.z + x.z, sum.w + x.w);
+        const uint32_t L = __ballot_sync(~0u, lead);
+        if (lead) lstage[__popc(L & lanemask_lt())] = (uint32_t)lane;
+        __syncwarp();
+        const int nl = __popc(L);
+        for (int i0 = 0; i0 < nl; i0 += UPS) {
+          const int i = i0 + slot;
+          if (i < nl && act) {
+            const uint32_t u = lstage[i];
+            uint32_t members = gstage[u];
+            float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+            while (members) {
+              const int m = __ffs(members) - 1;
+              members &= members - 1u;
+              const float4 x = lds4(xs + m * a.ldr + col);
+              sum = make_float4(sum.x + x.x, sum.y + x.y, sum.z + x.z, sum.w + x.w);
+            }
+            emit(ustage[u].x, sum);
           }
-          atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)ustage[u].x * a.ldr + col), sum);
         }
       }
+      if (d >= 1 && lane == d - 1) nodeL += (uint32_t)__popc(M);
+      __syncwarp();
     }
-    if (d >= 1 && lane == d - 1) nodeL += (uint32_t)__popc(M);
-    __syncwarp();
+  }
+  if constexpr (HOT) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.nhot * a.ldr; i += blockDim.x) {
+      const float v = hacc[i];
+      if (v != 0.f) atomicAdd(a.out + (size_t)a.hot_rows[i / a.ldr] * a.ldr + i % a.ldr, v);
+    }
+  }
+}
+
+// Units per output row of a scatter walk (the ids of its level).
+__global__ void k_row_count(const uint32_t *ids, uint64_t n, uint32_t rows, uint32_t *count) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = ids[i];
+    if (r < rows) atomicAdd(count + r, 1u);
   }
 }
 
@@ -722,6 +768,9 @@ WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   a.out = out;
   a.sched = w.sched.get();
   a.counter = w.sched.get() ? w.sched.get() + (size_t)w.nchunks * (w.src + 1) : nullptr;
+  a.nhot = w.nhot;
+  a.hot_slot = w.hot_slot.get();
+  a.hot_rows = w.hot_rows.get();
   return a;
 }
 
@@ -774,13 +823,25 @@ void launch_contract(int vec, const WalkArgs &a, unsigned blocks, bool resident,
   ADATM_LAUNCH();
 }
 
+template <int W, FactorType FT, bool LEAF>
+void launch_scatter_w(const WalkArgs &a, unsigned blocks, cudaStream_t s) {
+  if (a.nhot > 0) {
+    // each block sums the hot rows once: as few blocks as fit at once
+    const size_t smem = kWarps * scatter_warp_bytes(a.ldr) + (size_t)a.nhot * a.ldr * sizeof(float);
+    blocks = std::min(blocks, resident_blocks(k_scatter<W, FT, LEAF, true>, 256, smem));
+    k_scatter<W, FT, LEAF, true><<<blocks, 256, smem, s>>>(a);
+  } else {
+    k_scatter<W, FT, LEAF, false><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a);
+  }
+}
+
 template <FactorType FT, bool LEAF>
 void launch_scatter(int w, const WalkArgs &a, unsigned blocks, cudaStream_t s) {
   switch (w) {
-    case 4: k_scatter<4, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
-    case 8: k_scatter<8, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
-    case 16: k_scatter<16, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
-    case 32: k_scatter<32, FT, LEAF><<<blocks, 256, kWarps * scatter_warp_bytes(a.ldr), s>>>(a); break;
+    case 4: launch_scatter_w<4, FT, LEAF>(a, blocks, s); break;
+    case 8: launch_scatter_w<8, FT, LEAF>(a, blocks, s); break;
+    case 16: launch_scatter_w<16, FT, LEAF>(a, blocks, s); break;
+    case 32: launch_scatter_w<32, FT, LEAF>(a, blocks, s); break;
     default: throw BadInput("unsupported lanes per unit");
   }
   ADATM_LAUNCH();
@@ -816,9 +877,13 @@ void set_walk_attributes() {
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)contract_smem<V>(kMaxModes)));
 #define ADATM_ATTR_S(W, FT, LEAF)                                                 \
-  ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF>,                         \
+  ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF, false>,                  \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                  (int)(kWarps * scatter_warp_bytes(128))));
+                                  (int)(kWarps * scatter_warp_bytes(128))));      \
+  ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF, true>,                   \
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
+                                  (int)(kWarps * scatter_warp_bytes(128) +        \
+                                        kHotRows * 128 * sizeof(float))));
 #define ADATM_ATTR_ALL(M, X)                \
   M(X, FactorType::F32, true)               \
   M(X, FactorType::F32, false)              \
@@ -837,6 +902,41 @@ void set_walk_attributes() {
   done = true;
 }
 
+// The output rows of a scatter walk hit by the most units (at most
+// kHotRows, each by at least kHotMin units), and the row -> slot table.
+void find_hot_rows(TreeWalk &w, cudaStream_t s) {
+  const DevCsf &c = *w.csf;
+  const uint64_t rows64 = c.dims[c.dim_perm[w.out]];
+  if (rows64 == 0 || rows64 > 0xFFFFFFFFull) return;
+  const uint32_t rows = (uint32_t)rows64;
+  DevBuf<uint32_t> count(rows);
+  ADATM_CUDA(cudaMemsetAsync(count.get(), 0, rows * sizeof(uint32_t), s));
+  const unsigned blocks = (unsigned)std::min<uint64_t>((w.nunits + 255) / 256, 4096);
+  k_row_count<<<blocks, 256, 0, s>>>(c.fids[w.out].get(), w.nunits, rows, count.get());
+  ADATM_LAUNCH();
+  std::vector<uint32_t> h(rows);
+  ADATM_CUDA(cudaMemcpyAsync(h.data(), count.get(), rows * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  ADATM_CUDA(cudaStreamSynchronize(s));
+  std::vector<uint32_t> order(rows);
+  for (uint32_t r = 0; r < rows; ++r) order[r] = r;
+  const uint32_t k = std::min<uint32_t>(kHotRows, rows);
+  std::partial_sort(order.begin(), order.begin() + k, order.end(),
+                    [&](uint32_t x, uint32_t y) { return h[x] > h[y] || (h[x] == h[y] && x < y); });
+  std::vector<uint32_t> hot;
+  for (uint32_t i = 0; i < k; ++i)
+    if (h[order[i]] >= kHotMin) hot.push_back(order[i]);
+  if (hot.empty()) return;
+  std::vector<uint8_t> slot(rows, 0xFF);
+  for (size_t i = 0; i < hot.size(); ++i) slot[hot[i]] = (uint8_t)i;
+  w.hot_slot.alloc(rows);
+  w.hot_rows.alloc(hot.size());
+  ADATM_CUDA(cudaMemcpyAsync(w.hot_slot.get(), slot.data(), rows, cudaMemcpyHostToDevice, s));
+  ADATM_CUDA(cudaMemcpyAsync(w.hot_rows.get(), hot.data(), hot.size() * sizeof(uint32_t),
+                             cudaMemcpyHostToDevice, s));
+  ADATM_CUDA(cudaStreamSynchronize(s));
+  w.nhot = (int)hot.size();
+}
+
 void walk_prepare(TreeWalk &w, cudaStream_t s) {
   set_walk_attributes();
   const DevCsf &c = *w.csf;
@@ -845,10 +945,14 @@ void walk_prepare(TreeWalk &w, cudaStream_t s) {
   if (w.chunk == 0) w.chunk = 32;
   w.nchunks = (uint32_t)((w.nunits + w.chunk - 1) / w.chunk);
   w.sched.alloc((size_t)std::max<uint32_t>(w.nchunks, 1) * (w.src + 1) + 1);  // + the chunk counter
+  w.nhot = 0;
+  w.hot_slot.reset();
+  w.hot_rows.reset();
   if (w.nchunks == 0) return;
   WalkArgs a = make_args(w, nullptr, nullptr);
   k_schedule<<<(w.nchunks + 255) / 256, 256, 0, s>>>(a, w.sched.get());
   ADATM_LAUNCH();
+  if (w.src == w.out && w.nunits >= kHotMin) find_hot_rows(w, s);
 }
 
 void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float *out,

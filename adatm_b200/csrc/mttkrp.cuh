@@ -49,6 +49,12 @@ struct TreeWalk {
   DevBuf<uint32_t> sched;                    // nchunks x (S + 1), then the chunk counter
   bool resident = true;                      // contraction grid: resident blocks that claim
                                              // chunks (else one chunk per warp)
+  // Scatter walks: the output rows that the most units hit (at most
+  // kHotRows, each hit by at least kHotMin units) are summed per block in
+  // shared memory; hot_slot maps an output row to its slot (0xFF = none).
+  int nhot = 0;
+  DevBuf<uint8_t> hot_slot;
+  DevBuf<uint32_t> hot_rows;
   bool has_store() const {
     for (int l = 0; l < kMaxModes; ++l)
       if (store[l]) return true;

@@ -254,6 +254,11 @@ int adatm_engine_fit(adatm_engine *e, double *fit);
  * rows, the tree that feeds the last mode (whose MTTKRP gives the fit's
  * inner product) still reads FP32 rows. */
 int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes);
+/* Output rows that the mode's MTTKRP walk sums per block in shared memory
+ * before adding them to the output (rows hit by very many units of a scatter
+ * walk; 0 for contraction walks and unskewed outputs). Diagnostic; no
+ * reference counterpart. */
+int adatm_engine_hot_rows(adatm_engine *e, uint64_t mode, int *nhot);
 /* ------------------------------------------------------------------------ */
 /* Batched sweeps of many tensors and the chunk autotuner                   */
 /* ------------------------------------------------------------------------ */
