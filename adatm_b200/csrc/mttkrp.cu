@@ -33,6 +33,7 @@ struct WalkArgs {
 
 constexpr int kHotRows = 32;     // output rows summed per block, at most
 constexpr uint32_t kHotMin = 32768;  // units that must hit a row to make it one
+constexpr uint64_t kHotScanRows = 1ull << 24;  // output rows the hot-row search examines, at most
 
 // ---------------------------------------------------------------------------
 // Warp-uniform tree walk.
@@ -907,7 +908,9 @@ void set_walk_attributes() {
 void find_hot_rows(TreeWalk &w, cudaStream_t s) {
   const DevCsf &c = *w.csf;
   const uint64_t rows64 = c.dims[c.dim_perm[w.out]];
-  if (rows64 == 0 || rows64 > 0xFFFFFFFFull) return;
+  // a count per output row, on the device and the host: outputs with more
+  // rows than kHotScanRows keep the plain scatter
+  if (rows64 == 0 || rows64 > kHotScanRows) return;
   const uint32_t rows = (uint32_t)rows64;
   DevBuf<uint32_t> count(rows);
   ADATM_CUDA(cudaMemsetAsync(count.get(), 0, rows * sizeof(uint32_t), s));
