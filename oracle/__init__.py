@@ -67,10 +67,12 @@ _ref = None
 
 
 def build(ref_dir: str | None = None) -> None:
-    """Compile liboracle.so and, when the reference checkout exists, _ref."""
+    """Compile liboracle.so and, when a reference checkout is given (the
+    argument, else the ADATM_REFERENCE_DIR environment variable) and exists,
+    _ref/libadatm_ref.so from its sources."""
     subprocess.check_call(["make", "-s", "liboracle.so"], cwd=HERE)
-    ref = ref_dir or "/root/reference"
-    if os.path.isdir(os.path.join(ref, "src")):
+    ref = ref_dir or os.environ.get("ADATM_REFERENCE_DIR")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         subprocess.check_call(["make", "-s", "ref", f"REF={ref}"], cwd=HERE)
 
 
@@ -110,6 +112,15 @@ def lib():
         L.orc_cpd_als.argtypes = [C.c_void_p, C.POINTER(C.POINTER(OrcCsf)), u64,
                                   C.POINTER(P_f64), P_f64, u64, C.c_double, P_f64, P_u64]
         L.orc_cpd_als.restype = C.c_double
+        L.orc_generate.argtypes = [C.c_int, P_u64, u64, P_f64, C.c_int, C.c_double, C.c_double,
+                                   u64, P_u64, P_f64]
+        L.orc_mttkrp_coo.argtypes = [C.c_int, u64, P_u64, P_u64, P_f64, C.POINTER(P_f64), u64, u64,
+                                     P_f64]
+        L.orc_cpd_als_coo.argtypes = [C.c_int, u64, P_u64, P_u64, P_f64, u64, C.POINTER(P_f64),
+                                      P_f64, u64, C.c_double, P_f64, P_u64]
+        L.orc_cpd_als_coo.restype = C.c_double
+        L.orc_threads.argtypes = [C.c_int]
+        L.orc_threads.restype = C.c_int
         _lib = L
     return _lib
 
@@ -357,6 +368,64 @@ def _cpd(handle, plain, R, mats, niters, tol):
             "trace": trace[: done.value].copy(), "iters": int(done.value)}
 
 
+def threads(n=0):
+    """OpenMP threads of the parallel oracle paths (n > 0 sets them)."""
+    return int(lib().orc_threads(int(n)))
+
+
+def generate(dims, nnz, alpha=None, value_kind=0, mu=0.0, sigma=1.0, seed=0, clean=True):
+    """The seeded synthetic tensor of the library's device generator, made on
+    the host: (inds N x nnz uint64, vals, dims). With clean, duplicates are
+    summed and empty slices compacted (orc_coo_clean), as the library does
+    after generating."""
+    N = len(dims)
+    d = np.ascontiguousarray(dims, dtype=np.uint64).copy()
+    a = np.zeros(N) if alpha is None else np.ascontiguousarray(
+        [alpha] * N if np.isscalar(alpha) else alpha, dtype=np.float64)
+    inds = np.empty((N, int(nnz)), dtype=np.uint64)
+    vals = np.empty(int(nnz), dtype=np.float64)
+    lib().orc_generate(N, d.ctypes.data_as(P_u64), int(nnz), a.ctypes.data_as(P_f64), int(value_kind),
+                       float(mu), float(sigma), int(seed), inds.ctypes.data_as(P_u64),
+                       vals.ctypes.data_as(P_f64))
+    if not clean:
+        return inds, vals, [int(x) for x in d]
+    # clean in place (the arrays are ours): no copies of a large draw
+    n = lib().orc_coo_clean(N, int(nnz), d.ctypes.data_as(P_u64), inds.ctypes.data_as(P_u64),
+                            vals.ctypes.data_as(P_f64))
+    flat = inds.reshape(-1)[: N * n].reshape(N, n)
+    return flat, vals[:n], [int(x) for x in d]
+
+
+def mttkrp_coo(inds, vals, dims, mats, mode, nfactors):
+    """FP64 MTTKRP of `mode` from the coordinates (OpenMP)."""
+    inds = np.ascontiguousarray(inds, dtype=np.uint64)
+    N, nnz = inds.shape
+    d, dp = _u64(dims)
+    v, vp = _f64(vals)
+    keep, arr = _mats_ptrs(mats)
+    out = np.zeros((int(dims[mode]), nfactors), dtype=np.float64)
+    lib().orc_mttkrp_coo(N, nnz, dp, inds.ctypes.data_as(P_u64), vp, arr, mode, nfactors,
+                         out.ctypes.data_as(P_f64))
+    return out
+
+
+def cpd_als_coo(inds, vals, dims, nfactors, mats, niters, tol):
+    """CP-ALS with the FP64 COO MTTKRP (the same ALS steps as Model.cpd_als)."""
+    inds = np.ascontiguousarray(inds, dtype=np.uint64)
+    N, nnz = inds.shape
+    d, dp = _u64(dims)
+    v, vp = _f64(vals)
+    keep, arr = _mats_ptrs([np.array(m, dtype=np.float64, copy=True) for m in mats])
+    lam = np.zeros(nfactors, dtype=np.float64)
+    trace = np.zeros(max(1, niters), dtype=np.float64)
+    done = u64(0)
+    fit = lib().orc_cpd_als_coo(N, nnz, dp, inds.ctypes.data_as(P_u64), vp, nfactors, arr,
+                                lam.ctypes.data_as(P_f64), niters, tol,
+                                trace.ctypes.data_as(P_f64), C.byref(done))
+    return {"fit": fit, "lambda": lam, "factors": keep,
+            "trace": trace[: done.value].copy(), "iters": int(done.value)}
+
+
 def cpd_als_plain(inds, vals, dims, nfactors, mats, niters, tol):
     """CP-ALS with one plain CSF per mode (SPLATT_CSF_ALLMODE)."""
     inds = np.ascontiguousarray(inds, dtype=np.uint64)
@@ -394,6 +463,7 @@ def ref():
         L.ref_n_csf.argtypes = [C.c_void_p]
         L.ref_n_csf.restype = u64
         L.ref_use.argtypes = [C.c_void_p, P_u64, P_u64]
+        L.ref_set_use.argtypes = [C.c_void_p, P_u64, P_u64]
         L.ref_csf_shape.argtypes = [C.c_void_p, C.c_int, P_u64, P_u64]
         L.ref_csf_array.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, P_u64]
         L.ref_csf_array.restype = C.c_int
@@ -464,6 +534,12 @@ class RefModel:
         ut = np.zeros(self.N, dtype=np.uint64)
         ref().ref_use(self._h, uc.ctypes.data_as(P_u64), ut.ctypes.data_as(P_u64))
         return uc, ut
+
+    def set_use(self, use_csfs, use_tags):
+        """Per-mode trees and tags passed to the reference from now on."""
+        uc, ucp = _u64(use_csfs)
+        ut, utp = _u64(use_tags)
+        ref().ref_set_use(self._h, ucp, utp)
 
     def csf(self, g):
         N = self.N

@@ -21,6 +21,13 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
 
 #define ORC_ALLOC(T, n) ((T *)calloc((size_t)((n) > 0 ? (n) : 1), sizeof(T)))
 
@@ -970,41 +977,50 @@ static void orc_normalize(double *A, uint64_t I, uint64_t R, double *lambda,
     for (uint64_t r = 0; r < R; ++r) A[i * R + r] /= lambda[r];
 }
 
+/* MTTKRP of one mode through a caller-chosen method (the memoized model,
+ * a plain tree per mode, or the COO loop below). */
+typedef void (*orc_mttkrp_fn)(void *ctx, double *const *mats, uint64_t mode, double *out);
+
+typedef struct orc_plain_ctx {
+  const orc_csf *const *csfs;
+  uint64_t R;
+} orc_plain_ctx;
+
+static void orc_mttkrp_model_cb(void *ctx, double *const *mats, uint64_t mode, double *out) {
+  orc_mttkrp_adaptive((orc_model *)ctx, mats, mode, out);
+}
+
+static void orc_mttkrp_plain_cb(void *ctx, double *const *mats, uint64_t mode, double *out) {
+  orc_plain_ctx const *p = (orc_plain_ctx const *)ctx;
+  orc_mttkrp_csf(p->csfs[mode], mats, mode, p->R, out);
+}
+
 /* cpd_als_iterate_adaptive (adatm_cpd.c:256-373) with p_calc_fit
  * (adatm_cpd.c:179-200), p_kruskal_norm (:59-90) and p_tt_kruskal_inner
  * (:109-160), followed by cpd_post_process (SPLATT, :364): every factor is
- * 2-normalised and lambda absorbs the norms. With md == NULL the MTTKRPs
- * run on plain_csfs[m], a tree rooted at mode m (SPLATT_CSF_ALLMODE).
- * mats[m] (dims[m] x R, row-major) hold the initial factors on entry and the
- * final factors on return. Returns the last fit. */
-double orc_cpd_als(orc_model *md, const orc_csf *const *plain_csfs,
-                   uint64_t nfactors, double *const *mats, double *lambda,
-                   uint64_t niters, double tol, double *fit_trace,
-                   uint64_t *iters_done) {
-  orc_csf const *c0 = md ? md->csf[0] : plain_csfs[0];
-  int const N = c0->nmodes;
-  uint64_t const R = nfactors;
+ * 2-normalised and lambda absorbs the norms. The MTTKRP of each mode comes
+ * from `mttkrp`. mats[m] (dims[m] x R, row-major) hold the initial factors
+ * on entry and the final factors on return. Returns the last fit. */
+static double orc_als_core(int N, const uint64_t *dims, double ttnormsq, uint64_t R,
+                           orc_mttkrp_fn mttkrp, void *ctx, double *const *mats,
+                           double *lambda, uint64_t niters, double tol,
+                           double *fit_trace, uint64_t *iters_done) {
   uint64_t maxdim = 0;
   for (int m = 0; m < N; ++m)
-    if (c0->dims[m] > maxdim) maxdim = c0->dims[m];
+    if (dims[m] > maxdim) maxdim = dims[m];
   double *G[ORC_MAXN];
   for (int m = 0; m < N; ++m) {
     G[m] = ORC_ALLOC(double, R * R);
-    orc_ata(mats[m], c0->dims[m], R, G[m]);
+    orc_ata(mats[m], dims[m], R, G[m]);
   }
   double *Vinv = ORC_ALLOC(double, R * R);
   double *M = ORC_ALLOC(double, maxdim * R);
-  double ttnormsq = 0;
-  for (uint64_t n = 0; n < c0->nnz; ++n) ttnormsq += c0->vals[n] * c0->vals[n];
   double fit = 0, oldfit = 0;
   uint64_t it = 0;
   for (it = 0; it < niters; ++it) {
     for (int m = 0; m < N; ++m) {
-      uint64_t const I = c0->dims[m];
-      if (md)
-        orc_mttkrp_adaptive(md, mats, (uint64_t)m, M);
-      else
-        orc_mttkrp_csf(plain_csfs[m], mats, (uint64_t)m, R, M);
+      uint64_t const I = dims[m];
+      mttkrp(ctx, mats, (uint64_t)m, M);
       orc_gram_inv(G, N, (uint64_t)m, R, Vinv);
       double *A = mats[m];
       for (uint64_t i = 0; i < I; ++i)
@@ -1028,7 +1044,7 @@ double orc_cpd_als(orc_model *md, const orc_csf *const *plain_csfs,
     /* p_tt_kruskal_inner: M holds the last mode's MTTKRP */
     double inner = 0;
     {
-      uint64_t const I = c0->dims[N - 1];
+      uint64_t const I = dims[N - 1];
       const double *A = mats[N - 1];
       for (uint64_t r = 0; r < R; ++r) {
         double acc = 0;
@@ -1049,7 +1065,7 @@ double orc_cpd_als(orc_model *md, const orc_csf *const *plain_csfs,
   /* cpd_post_process */
   double *tmp = ORC_ALLOC(double, R);
   for (int m = 0; m < N; ++m) {
-    orc_normalize(mats[m], c0->dims[m], R, tmp, 2);
+    orc_normalize(mats[m], dims[m], R, tmp, 2);
     for (uint64_t r = 0; r < R; ++r) lambda[r] *= tmp[r];
   }
   free(tmp);
@@ -1057,4 +1073,170 @@ double orc_cpd_als(orc_model *md, const orc_csf *const *plain_csfs,
   free(Vinv);
   free(M);
   return fit;
+}
+
+/* CP-ALS on the memoized model md, or with md == NULL on plain_csfs[m], a
+ * tree rooted at mode m (SPLATT_CSF_ALLMODE). See orc_als_core. */
+double orc_cpd_als(orc_model *md, const orc_csf *const *plain_csfs,
+                   uint64_t nfactors, double *const *mats, double *lambda,
+                   uint64_t niters, double tol, double *fit_trace,
+                   uint64_t *iters_done) {
+  orc_csf const *c0 = md ? md->csf[0] : plain_csfs[0];
+  double ttnormsq = 0;
+  for (uint64_t n = 0; n < c0->nnz; ++n) ttnormsq += c0->vals[n] * c0->vals[n];
+  orc_plain_ctx pc = {plain_csfs, nfactors};
+  return orc_als_core(c0->nmodes, c0->dims, ttnormsq, nfactors,
+                      md ? orc_mttkrp_model_cb : orc_mttkrp_plain_cb,
+                      md ? (void *)md : (void *)&pc, mats, lambda, niters, tol,
+                      fit_trace, iters_done);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic tensors and an FP64 path for large cases                */
+/* ------------------------------------------------------------------------ */
+
+/* Seeded draws with the shapes the benchmark configurations name, the same
+ * numbers the library's device generator produces: coordinate m of draw i
+ * comes from u = mix64(key_m + i) >> 11 scaled by 2^-53, key_m =
+ * mix64(seed * 0x100000001B3 + 0x1000 + m); uniform indices are
+ * floor(u * dim), Zipf(alpha) indices the smallest k with u < CDF(k) for
+ * P(k) proportional to (k+1)^-alpha; values are u01 of key_N (uniform) or
+ * exp(mu + sigma * z) with the Box-Muller z of keys N and N+1 (lognormal).
+ * Duplicates are kept (orc_coo_clean sums them). inds is mode-major
+ * (nmodes x nnz). Indices and uniform values are bit-identical to the device
+ * generator's; lognormal values agree to within a few ulps (the device's
+ * cos(pi x), exp and log round differently from glibc's). */
+void orc_generate(int nmodes, const uint64_t *dims, uint64_t nnz, const double *alpha,
+                  int value_kind, double mu, double sigma, uint64_t seed, uint64_t *inds,
+                  double *vals) {
+  uint64_t key[ORC_MAXN + 2];
+  double *cdf[ORC_MAXN];
+  for (int m = 0; m < nmodes + 2; ++m) key[m] = orc_mix64(seed * 0x100000001B3ull + 0x1000u + (uint64_t)m);
+  for (int m = 0; m < nmodes; ++m) {
+    cdf[m] = NULL;
+    if (alpha && alpha[m] > 0) {
+      cdf[m] = ORC_ALLOC(double, dims[m]);
+      double acc = 0;
+      for (uint64_t k = 0; k < dims[m]; ++k) {
+        acc += pow((double)(k + 1), -alpha[m]);
+        cdf[m][k] = acc;
+      }
+      for (uint64_t k = 0; k < dims[m]; ++k) cdf[m][k] /= acc;
+      cdf[m][dims[m] - 1] = 1.0;
+    }
+  }
+  const double scale = 1.0 / 9007199254740992.0;
+#pragma omp parallel for schedule(static)
+  for (int64_t ii = 0; ii < (int64_t)nnz; ++ii) {
+    uint64_t const i = (uint64_t)ii;
+    for (int m = 0; m < nmodes; ++m) {
+      double const u = (double)(orc_mix64(key[m] + i) >> 11) * scale;
+      uint64_t k;
+      if (cdf[m] == NULL) {
+        k = (uint64_t)(u * (double)dims[m]);
+        if (k >= dims[m]) k = dims[m] - 1;
+      } else {
+        uint64_t lo = 0, hi = dims[m] - 1;
+        while (lo < hi) {
+          uint64_t const mid = (lo + hi) >> 1;
+          if (u < cdf[m][mid])
+            hi = mid;
+          else
+            lo = mid + 1;
+        }
+        k = lo;
+      }
+      inds[(uint64_t)m * nnz + i] = k;
+    }
+    double const u1 = (double)(orc_mix64(key[nmodes] + i) >> 11) * scale;
+    if (value_kind == 0) {
+      vals[i] = u1;
+    } else {
+      double const u2 = (double)(orc_mix64(key[nmodes + 1] + i) >> 11) * scale;
+      double const z = sqrt(-2.0 * log(1.0 - u1)) * cos(2.0 * M_PI * u2);
+      vals[i] = exp(mu + sigma * z);
+    }
+  }
+  for (int m = 0; m < nmodes; ++m) free(cdf[m]);
+}
+
+/* MTTKRP of `mode` straight from the coordinates:
+ * out[i_mode(n)] += v_n * prod_{m != mode} U_m[i_m(n)], the quantity every
+ * CSF kernel of the reference computes (mttkrp.c:241-1682) summed in another
+ * order. OpenMP threads take static contiguous ranges of nonzeros into
+ * private rows, summed in thread order afterwards, so a run repeats bit for
+ * bit at a fixed thread count. */
+void orc_mttkrp_coo(int nmodes, uint64_t nnz, const uint64_t *dims, const uint64_t *inds,
+                    const double *vals, double *const *mats, uint64_t mode, uint64_t R,
+                    double *out) {
+  uint64_t const I = dims[mode];
+  memset(out, 0, I * R * sizeof(double));
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  double *priv = ORC_ALLOC(double, (uint64_t)nt * I * R);
+#pragma omp parallel num_threads(nt)
+  {
+    int t = 0;
+#ifdef _OPENMP
+    t = omp_get_thread_num();
+#endif
+    double *o = priv + (uint64_t)t * I * R;
+    double *row = ORC_ALLOC(double, R);
+    uint64_t const lo = nnz * (uint64_t)t / (uint64_t)nt, hi = nnz * (uint64_t)(t + 1) / (uint64_t)nt;
+    for (uint64_t n = lo; n < hi; ++n) {
+      for (uint64_t r = 0; r < R; ++r) row[r] = vals[n];
+      for (int m = 0; m < nmodes; ++m) {
+        if ((uint64_t)m == mode) continue;
+        const double *U = mats[m] + inds[(uint64_t)m * nnz + n] * R;
+        for (uint64_t r = 0; r < R; ++r) row[r] *= U[r];
+      }
+      double *dst = o + inds[mode * nnz + n] * R;
+      for (uint64_t r = 0; r < R; ++r) dst[r] += row[r];
+    }
+    free(row);
+  }
+#pragma omp parallel for schedule(static)
+  for (int64_t x = 0; x < (int64_t)(I * R); ++x) {
+    double s = 0;
+    for (int t = 0; t < nt; ++t) s += priv[(uint64_t)t * I * R + (uint64_t)x];
+    out[x] = s;
+  }
+  free(priv);
+}
+
+typedef struct orc_coo_ctx {
+  int nmodes;
+  uint64_t nnz, R;
+  const uint64_t *dims, *inds;
+  const double *vals;
+} orc_coo_ctx;
+
+static void orc_mttkrp_coo_cb(void *ctx, double *const *mats, uint64_t mode, double *out) {
+  orc_coo_ctx const *c = (orc_coo_ctx const *)ctx;
+  orc_mttkrp_coo(c->nmodes, c->nnz, c->dims, c->inds, c->vals, mats, mode, c->R, out);
+}
+
+/* CP-ALS (orc_als_core) with the COO MTTKRP: the FP64 reference run for
+ * tensors too large for the single-threaded tree restatement. */
+double orc_cpd_als_coo(int nmodes, uint64_t nnz, const uint64_t *dims, const uint64_t *inds,
+                       const double *vals, uint64_t nfactors, double *const *mats,
+                       double *lambda, uint64_t niters, double tol, double *fit_trace,
+                       uint64_t *iters_done) {
+  double ttnormsq = 0;
+  for (uint64_t n = 0; n < nnz; ++n) ttnormsq += vals[n] * vals[n];
+  orc_coo_ctx c = {nmodes, nnz, nfactors, dims, inds, vals};
+  return orc_als_core(nmodes, dims, ttnormsq, nfactors, orc_mttkrp_coo_cb, &c, mats, lambda,
+                      niters, tol, fit_trace, iters_done);
+}
+
+int orc_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
 }

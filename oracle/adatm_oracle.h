@@ -117,4 +117,20 @@ double orc_cpd_als(orc_model *md, const orc_csf *const *plain_csfs,
                    uint64_t niters, double tol, double *fit_trace,
                    uint64_t *iters_done);
 
+
+/* --- seeded synthetic tensors; FP64 COO path for large cases ------------- */
+void orc_generate(int nmodes, const uint64_t *dims, uint64_t nnz, const double *alpha,
+                  int value_kind, double mu, double sigma, uint64_t seed, uint64_t *inds,
+                  double *vals);
+void orc_mttkrp_coo(int nmodes, uint64_t nnz, const uint64_t *dims, const uint64_t *inds,
+                    const double *vals, double *const *mats, uint64_t mode, uint64_t R,
+                    double *out);
+double orc_cpd_als_coo(int nmodes, uint64_t nnz, const uint64_t *dims, const uint64_t *inds,
+                       const double *vals, uint64_t nfactors, double *const *mats,
+                       double *lambda, uint64_t niters, double tol, double *fit_trace,
+                       uint64_t *iters_done);
+/* OpenMP threads of the parallel oracle paths (n > 0 sets them); returns
+ * the count in use. */
+int orc_threads(int n);
+
 #endif

@@ -157,6 +157,15 @@ ref_state *ref_build(int N, uint64_t nnz, const uint64_t *dims,
 
 uint64_t ref_n_csf(ref_state *st) { return st->n_csf; }
 
+/* Replace the per-mode trees and tags that ref_mttkrp / ref_cpd pass to the
+ * reference (a caller's own use_csfs / use_tags instead of decide_use_csfs's). */
+void ref_set_use(ref_state *st, const uint64_t *use_csfs, const uint64_t *use_tags) {
+  for (idx_t m = 0; m < st->tt.nmodes; ++m) {
+    st->use_csfs[m] = use_csfs[m];
+    st->use_tags[m] = use_tags[m];
+  }
+}
+
 void ref_use(ref_state *st, uint64_t *use_csfs, uint64_t *use_tags) {
   for (idx_t m = 0; m < st->tt.nmodes; ++m) {
     use_csfs[m] = st->use_csfs[m];

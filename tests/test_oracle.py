@@ -128,3 +128,57 @@ def test_empty_and_single_nonzero_csf():
     assert list(c["nfibs"]) == [1, 1, 1]
     assert list(c["fptr"][0]) == [0, 1] and list(c["fptr"][1]) == [0, 1]
     assert list(c["fids"][2]) == [0] and c["vals"][0] == 2.5
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_coo_path_matches_tree_restatement(name):
+    """The OpenMP COO MTTKRP and the ALS built on it (the FP64 reference run
+    for full-size workloads) equal the tree restatement, which the golden
+    fixtures pin to the reference's own code."""
+    d = load_golden(name)
+    N, R = d["N"], int(d["R"])
+    md = O.Model(d["inds"], d["vals"], d["dims_list"], R, d["groups"])
+    mats = O.init_factors(d["dims_list"], R, 0)
+    for m in range(N):
+        a = md.mttkrp(mats, m)
+        b = O.mttkrp_coo(d["inds"], d["vals"], d["dims_list"], mats, m, R)
+        assert np.max(np.abs(a - b)) <= 1e-12 * np.max(np.abs(a))
+    r1 = md.cpd_als(mats, 5, 0.0)
+    r2 = O.cpd_als_coo(d["inds"], d["vals"], d["dims_list"], R, mats, 5, 0.0)
+    assert abs(r1["fit"] - r2["fit"]) < 1e-12
+    assert abs(r2["fit"] - float(d["als5_fit"])) < 1e-10
+    np.testing.assert_allclose(r2["lambda"], r1["lambda"], rtol=1e-9)
+
+
+def test_coo_path_repeats_at_fixed_threads():
+    inds, vals, dims = O.generate([300, 200, 100, 50], 200_000, alpha=1.2, seed=5)
+    mats = O.init_factors(dims, 8, 1)
+    a = O.mttkrp_coo(inds, vals, dims, mats, 2, 8)
+    b = O.mttkrp_coo(inds, vals, dims, mats, 2, 8)
+    assert a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("alpha,kind", [(None, 0), (1.1, 0), (1.3, 1)])
+def test_host_generator(alpha, kind):
+    """The host port of the seeded generator: shapes, bounds, cleaned (no
+    duplicates, no empty slices), deterministic; Zipf skews towards index 0;
+    lognormal values are positive with log-mean near 0."""
+    dims = [400, 300, 200, 100]
+    inds, vals, d = O.generate(dims, 300_000, alpha=alpha, value_kind=kind, seed=11)
+    i2, v2, d2 = O.generate(dims, 300_000, alpha=alpha, value_kind=kind, seed=11)
+    assert d == d2 and inds.tobytes() == i2.tobytes() and vals.tobytes() == v2.tobytes()
+    N, nnz = inds.shape
+    for m in range(N):
+        assert inds[m].max() < d[m] and len(np.unique(inds[m])) == d[m]
+    keys = np.zeros(nnz, dtype=np.uint64)
+    for m in range(N):
+        keys = keys * np.uint64(dims[m]) + inds[m]
+    assert len(np.unique(keys)) == nnz
+    raw, rv, _ = O.generate(dims, 300_000, alpha=alpha, value_kind=kind, seed=11, clean=False)
+    assert raw.shape == (N, 300_000) and abs(rv.sum() - vals.sum()) < 1e-9 * abs(rv.sum())
+    if alpha:
+        assert np.mean(raw[0] == 0) > 5 * np.mean(raw[0] == 50)
+    if kind == 1:
+        assert rv.min() > 0 and abs(np.mean(np.log(rv))) < 0.01
+    else:
+        assert rv.min() >= 0 and rv.max() < 1
