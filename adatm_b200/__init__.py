@@ -308,6 +308,8 @@ def mttkrp_csf_adaptive(csf: CsfSet, rcsf: RcsfSet, mats, mode, groups, use_csfs
     lib().mttkrp_csf_adaptive(csf.ptr, rcsf.ptr if rcsf else None, len(csf), arr, mode, None,
                               ga.arr, ga.n, int(use_csfs[mode]), int(use_tags[mode]),
                               opts.ctypes.data_as(C.POINTER(C.c_double)))
+    if N.last_error():
+        raise AdatmError(SPLATT_ERROR_BADINPUT, "mttkrp_csf_adaptive")
     return out[: mats[mode].shape[0]].copy()
 
 
@@ -325,6 +327,8 @@ def cpd_als_iterate_adaptive(csf: CsfSet, rcsf: RcsfSet, groups, use_csfs, use_t
     fit = lib().cpd_als_iterate_adaptive(csf.ptr, rcsf.ptr if rcsf else None, len(csf), ga.arr, ga.n,
                                          ucp, utp, arr, lam.ctypes.data_as(C.POINTER(C.c_double)),
                                          R, None, opts.ctypes.data_as(C.POINTER(C.c_double)))
+    if N.last_error():
+        raise AdatmError(SPLATT_ERROR_BADINPUT, "cpd_als_iterate_adaptive")
     return {"fit": fit, "lambda": lam, "factors": keep}
 
 

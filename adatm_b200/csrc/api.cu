@@ -37,6 +37,7 @@ int fail(int code, const char *msg) {
 
 template <typename F>
 int guarded(F &&f) {
+  g_last_error.clear();
   try {
     f();
     return SPLATT_SUCCESS;
@@ -75,15 +76,29 @@ struct CsfHandle {
   Plan plan;
   splatt_csf *host = nullptr;
   int n_csf = 0;
-  std::map<uint64_t, std::unique_ptr<Engine>> engines;  // by rank
+  // engines by rank and group list (a caller may pass other memo levels
+  // for the same trees); each keeps its own factors and memo rows
+  std::map<std::string, std::unique_ptr<Engine>> engines;
   std::vector<rcsf_seq_adaptive *> memo_views;
+  // the handle's own plan, with its own trees and tags per mode
   Engine &engine(uint64_t R) {
-    auto it = engines.find(R);
+    Engine &e = engine(R, plan);
+    e.set_use(plan.use_csfs, plan.use_tags);
+    return e;
+  }
+  Engine &engine(uint64_t R, const Plan &p) {
+    std::string key = std::to_string(R) + (p.space_efficient ? "s" : "t");
+    for (int g = 0; g < p.n_grp; ++g) {
+      key += "|" + std::to_string(p.grp[g].memo_mode) + "," + std::to_string(p.grp[g].begin_imten) +
+             "," + std::to_string(p.grp[g].n_imten) + ":";
+      for (int l = 0; l < p.nmodes; ++l) key += std::to_string(p.grp[g].o_opt[l]) + ".";
+    }
+    auto it = engines.find(key);
     if (it != engines.end()) return *it->second;
     EngineOptions o;
-    auto e = std::make_unique<Engine>(coo, trees, R, plan, o, stream.s);
+    auto e = std::make_unique<Engine>(coo, trees, R, p, o, stream.s);
     Engine &ref = *e;
-    engines[R] = std::move(e);
+    engines[key] = std::move(e);
     return ref;
   }
 };
@@ -210,6 +225,68 @@ void check_plan(const Plan &p) {
   }
 }
 
+
+// The group list a reference caller passes with a call (grp_prop, n_grp and
+// n_csf, as csf_alloc_adaptive / decide_use_csfs read them), checked against
+// the trees the handle holds: the same number of trees, each in the level
+// order its group names. The memo levels (begin_imten, n_imten) may differ
+// from the handle's: they select the engine. With grp == nullptr the
+// handle's own plan. The memo sequences rs_seq (when given) must describe
+// the same memo levels as the groups.
+Plan caller_plan(const CsfHandle &h, const group_properties *grp, idx_t n_grp, idx_t n_csf,
+                 const rcsf_seq_adaptive *rs_seq) {
+  const int N = h.coo->nmodes;
+  if (n_csf != (idx_t)h.plan.n_csf)
+    throw BadInput("n_csf (" + std::to_string(n_csf) + ") is not the number of trees built (" +
+                   std::to_string(h.plan.n_csf) + ")");
+  Plan p = h.plan;
+  if (grp != nullptr) {
+    if (n_grp < 1 || n_grp > (idx_t)N) throw BadInput("n_grp out of range");
+    for (idx_t g = 0; g < n_grp; ++g)
+      if (grp[g].o_opt == nullptr) throw BadInput("grp_prop has a group without o_opt");
+    p = plan_from_groups(N, grp, n_grp, n_csf != n_grp);
+    check_plan(p);
+    if (p.n_csf != h.plan.n_csf)
+      throw BadInput("grp_prop describes a different number of trees than were built");
+    for (int t = 0; t < p.n_csf; ++t)
+      for (int l = 0; l < N; ++l)
+        if (p.tree(t).o_opt[l] != h.trees[t]->dim_perm[l])
+          throw BadInput("grp_prop's o_opt is not the level order of the trees these were built with");
+  }
+  if (rs_seq != nullptr) {
+    idx_t j = 0;
+    for (int t = 0; t < p.n_csf; ++t) {
+      const Group &gp = p.tree(t);
+      if (gp.n_imten == 0) continue;
+      if (rs_seq[j].begin_imten != gp.begin_imten || rs_seq[j].n_imten != gp.n_imten)
+        throw BadInput("rs_seq's memo levels differ from grp_prop's");
+      ++j;
+    }
+  }
+  return p;
+}
+
+// The engine of a reference caller's ALS call: its groups (memo levels) and
+// its per-mode trees and tags (use_csfs / use_tags, validated by set_use).
+Engine &caller_engine(CsfHandle &h, rcsf_seq_adaptive const *rs_seq, idx_t n_csf,
+                      group_properties const *grp_prop, idx_t n_grp, idx_t const *use_csfs,
+                      idx_t const *use_tags, uint64_t R) {
+  const Plan p = caller_plan(h, grp_prop, grp_prop ? n_grp : 0, n_csf, rs_seq);
+  Engine &e = h.engine(R, p);
+  if ((use_csfs == nullptr) != (use_tags == nullptr))
+    throw BadInput("use_csfs and use_tags must be given together");
+  if (use_csfs != nullptr) {
+    uint64_t uc[kMaxModes], ut[kMaxModes];
+    for (int m = 0; m < e.nmodes(); ++m) {
+      uc[m] = use_csfs[m];
+      ut[m] = use_tags[m];
+    }
+    e.set_use(uc, ut);
+  } else {
+    e.set_use(p.use_csfs, p.use_tags);
+  }
+  return e;
+}
 
 // The ALS loop shared by the splatt_* entry points, with the reference's
 // per-iteration report (adatm_cpd.c:343-354).
@@ -696,25 +773,22 @@ void mttkrp_csf_adaptive(splatt_csf const *const tensors, rcsf_seq_adaptive cons
                          thd_info *const thds, group_properties *const grp_prop,
                          int const n_grp, idx_t const use_csf, idx_t const use_tag,
                          double const *const opts) {
-  (void)rs_seq;
-  (void)n_csf;
   (void)thds;
-  (void)grp_prop;
-  (void)n_grp;
   (void)opts;
   int rc = guarded([&] {
     auto h = find_csf(tensors);
     const int N = h->coo->nmodes;
+    if (mode >= (idx_t)N) throw BadInput("mode out of range");
     const uint64_t R = mats[0]->J;
-    Engine &e = h->engine(R);
+    // the caller's groups pick the engine (memo levels); its tree and tag
+    // pick the walk, as the reference's dispatch does (mttkrp.c:2058-2087)
+    const Plan p = caller_plan(*h, grp_prop, grp_prop ? (idx_t)n_grp : 0, n_csf, rs_seq);
+    Engine &e = h->engine(R, p);
+    e.check_use((int)mode, (int)std::min<idx_t>(use_csf, kMaxModes), (int)std::min<idx_t>(use_tag, 3));
     const double *fm[kMaxModes];
     for (int m = 0; m < N; ++m) fm[m] = mats[m]->vals;
     e.set_factors(fm);
-    const bool as_planned = e.plan().use_csfs[mode] == use_csf && e.plan().use_tags[mode] == use_tag;
-    if (as_planned)
-      e.mttkrp((int)mode, e.mttkrp_buffer());
-    else
-      e.mttkrp_direct((int)mode, e.mttkrp_buffer());
+    e.mttkrp_with((int)mode, (int)use_csf, (int)use_tag, e.mttkrp_buffer());
     const uint64_t I = e.dims()[mode];
     std::vector<float> buf((size_t)I * e.ldr());
     ADATM_CUDA(cudaMemcpyAsync(buf.data(), e.mttkrp_buffer(), buf.size() * sizeof(float),
@@ -734,18 +808,12 @@ double cpd_als_iterate_adaptive(splatt_csf const *const tensors, rcsf_seq_adapti
                                 splatt_idx_t const *const use_tags, matrix_t **mats,
                                 val_t *const lambda, idx_t const nfactors,
                                 rank_info *const rinfo, double const *const opts) {
-  (void)rs_seq;
-  (void)n_csf;
-  (void)grp_prop;
-  (void)n_grp;
-  (void)use_csfs;
-  (void)use_tags;
   (void)rinfo;
   double fit = 0;
   int rc = guarded([&] {
     auto h = find_csf(tensors);
     const int N = h->coo->nmodes;
-    Engine &e = h->engine(nfactors);
+    Engine &e = caller_engine(*h, rs_seq, n_csf, grp_prop, n_grp, use_csfs, use_tags, nfactors);
     const double *fm[kMaxModes];
     double *om[kMaxModes];
     for (int m = 0; m < N; ++m) {
@@ -757,7 +825,10 @@ double cpd_als_iterate_adaptive(splatt_csf const *const tensors, rcsf_seq_adapti
                   (int)opts[SPLATT_OPTION_VERBOSITY]);
     e.get_normalized(om, lambda);
   });
-  if (rc != SPLATT_SUCCESS) fprintf(stderr, "cpd_als_iterate_adaptive: %s\n", g_last_error.c_str());
+  if (rc != SPLATT_SUCCESS) {
+    fprintf(stderr, "cpd_als_iterate_adaptive: %s\n", g_last_error.c_str());
+    fit = std::nan("");
+  }
   return fit;
 }
 
@@ -766,15 +837,9 @@ int splatt_cpd_als_adaptive(splatt_csf const *const tensors, rcsf_seq_adaptive *
                             splatt_idx_t const n_grp, splatt_idx_t const *const use_csfs,
                             splatt_idx_t const *const use_tags, splatt_idx_t const nfactors,
                             double const *const options, splatt_kruskal *factored) {
-  (void)rs_seq;
-  (void)n_csf;
-  (void)grp_prop;
-  (void)n_grp;
-  (void)use_csfs;
-  (void)use_tags;
   return guarded([&] {
     auto h = find_csf(tensors);
-    Engine &e = h->engine(nfactors);
+    Engine &e = caller_engine(*h, rs_seq, n_csf, grp_prop, n_grp, use_csfs, use_tags, nfactors);
     e.init_factors((uint64_t)options[SPLATT_OPTION_RANDSEED]);
     const double fit = run_als(e, (uint64_t)options[SPLATT_OPTION_NITER],
                                options[SPLATT_OPTION_TOLERANCE],

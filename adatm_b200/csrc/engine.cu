@@ -173,6 +173,7 @@ void Engine::set_resident_grid(bool on) {
     walk_[m]->resident = on;
     direct_[m]->resident = on;
   }
+  for (auto &kv : custom_) kv.second->resident = on;
 }
 
 float Engine::time_sweeps(int count) {
@@ -309,56 +310,119 @@ size_t Engine::csf_bytes() const {
   return b;
 }
 
-void Engine::build_walks() {
+// Memo levels a reuse MTTKRP of output level d can start from: the leading
+// stored levels of the group that lie below d (mttkrp.c:1578-1588 with
+// rcsf_reverse_mode_order, adatm_rcsf.c:313-326).
+static uint64_t reuse_indeg(const Group &gp, int d) {
+  const uint64_t b = gp.begin_imten;
+  uint64_t rd[kMaxModes + 1] = {0};
+  uint64_t j = 0;
+  for (int64_t i = (int64_t)b; i >= 0; --i)
+    if (i != d) rd[j++] = (uint64_t)i;
+  uint64_t indeg = 0;
+  for (uint64_t i = 0; i < gp.n_imten; ++i)
+    if (b - i == rd[i]) ++indeg;
+  return indeg;
+}
+
+void Engine::check_use(int mode, int tree, int tag) const {
   const int N = coo_->nmodes;
-  for (int m = 0; m < N; ++m) {
-    const int g = (int)plan_.use_csfs[m];
-    const int tag = (int)plan_.use_tags[m];
-    const DevCsf &c = *csf_[g];
-    const Group &gp = plan_.tree(g);
-    const int d = depth_of(c, m);
-    auto direct = std::make_unique<TreeWalk>();
-    direct->csf = &c;
-    direct->R = (int)R_;
-    direct->ldr = ldr_;
-    direct->src = N - 1;
-    direct->out = d;
-    direct->chunk = opt_.chunk_leaf;
-    direct->resident = opt_.resident_grid;
-    walk_prepare(*direct, stream_);
-    auto w = std::make_unique<TreeWalk>();
-    w->csf = &c;
-    w->R = (int)R_;
-    w->ldr = ldr_;
-    w->src = N - 1;
-    w->out = d;
-    w->chunk = opt_.chunk_leaf;
-    w->resident = opt_.resident_grid;
-    if (tag == 0 && gp.n_imten > 0) {
-      // memo root: store level begin_imten-1-deg into memo tree deg
-      for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
-        w->store[gp.begin_imten - 1 - deg] = memo_[g][deg].get();
-    } else if (tag == 1) {
-      // reuse: the leading memo levels that lie below the output level
-      // (mttkrp.c:1578-1588 with rcsf_reverse_mode_order, adatm_rcsf.c:313-326)
-      const uint64_t b = gp.begin_imten;
-      uint64_t rd[kMaxModes + 1] = {0};
-      uint64_t j = 0;
-      for (int64_t i = (int64_t)b; i >= 0; --i)
-        if (i != d) rd[j++] = (uint64_t)i;
-      uint64_t indeg = 0;
-      for (uint64_t i = 0; i < gp.n_imten; ++i)
-        if (b - i == rd[i]) ++indeg;
-      if (indeg > 0) {
-        w->src = (int)(b - indeg);
-        w->src_rows = memo_[g][indeg - 1].get();
-        w->chunk = opt_.chunk_rows;
-      }
-    }
-    walk_prepare(*w, stream_);
-    walk_[m] = std::move(w);
-    direct_[m] = std::move(direct);
+  if (mode < 0 || mode >= N) throw BadInput("mode out of range");
+  if (tree < 0 || tree >= (int)csf_.size()) throw BadInput("use_csfs names a tree that was not built");
+  const int d = depth_of(*csf_[tree], mode);
+  const Group &gp = plan_.tree(tree);
+  switch (tag) {
+    case 0:
+      if (d != 0) throw BadInput("use_tags 0 (root MTTKRP) on a mode that is not the tree's root");
+      break;
+    case 1:
+      if (gp.n_imten == 0) throw BadInput("use_tags 1 (memo reuse) on a tree whose group stores no memo rows");
+      // the reference indexes the memo sequence by indeg-1 (mttkrp.c:1591)
+      if (reuse_indeg(gp, d) == 0)
+        throw BadInput("use_tags 1 (memo reuse) on a mode whose level lies below every stored memo level");
+      break;
+    case 2:
+      if (d == 0) throw BadInput("use_tags 2 (recompute) on the tree's root mode");
+      break;
+    default: throw BadInput("use_tags must be 0, 1 or 2");
   }
+}
+
+std::unique_ptr<TreeWalk> Engine::make_walk(int mode, int g, int tag) {
+  const int N = coo_->nmodes;
+  const DevCsf &c = *csf_[g];
+  const Group &gp = plan_.tree(g);
+  const int d = depth_of(c, mode);
+  auto w = std::make_unique<TreeWalk>();
+  w->csf = &c;
+  w->R = (int)R_;
+  w->ldr = ldr_;
+  w->src = N - 1;
+  w->out = d;
+  w->chunk = opt_.chunk_leaf;
+  w->resident = opt_.resident_grid;
+  if (tag == 0 && gp.n_imten > 0) {
+    // memo root: store level begin_imten-1-deg into memo tree deg
+    for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
+      w->store[gp.begin_imten - 1 - deg] = memo_[g][deg].get();
+  } else if (tag == 1) {
+    const uint64_t indeg = reuse_indeg(gp, d);
+    if (indeg > 0) {
+      w->src = (int)(gp.begin_imten - indeg);
+      w->src_rows = memo_[g][indeg - 1].get();
+      w->chunk = opt_.chunk_rows;
+    }
+  }
+  walk_prepare(*w, stream_);
+  return w;
+}
+
+void Engine::build_walks() {
+  custom_.clear();
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    const int g = (int)plan_.use_csfs[m];
+    walk_[m] = make_walk(m, g, (int)plan_.use_tags[m]);
+    direct_[m] = make_walk(m, g, 2);
+  }
+}
+
+void Engine::set_use(const uint64_t *use_csfs, const uint64_t *use_tags) {
+  const int N = coo_->nmodes;
+  bool same = true;
+  for (int m = 0; m < N; ++m) {
+    check_use(m, (int)std::min<uint64_t>(use_csfs[m], kMaxModes),
+              (int)std::min<uint64_t>(use_tags[m], 3));
+    if (use_tags[m] == 1) {
+      bool root_before = false;
+      for (int k = 0; k < m; ++k) root_before |= use_csfs[k] == use_csfs[m] && use_tags[k] == 0;
+      if (!root_before)
+        throw BadInput("use_tags 1 (memo reuse) needs the root MTTKRP (tag 0) of the same tree at an "
+                       "earlier mode of the sweep");
+    }
+    same &= plan_.use_csfs[m] == use_csfs[m] && plan_.use_tags[m] == use_tags[m];
+  }
+  if (same) return;
+  drop_graph();
+  for (int m = 0; m < N; ++m) {
+    plan_.use_csfs[m] = use_csfs[m];
+    plan_.use_tags[m] = use_tags[m];
+  }
+  build_walks();
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::mttkrp_with(int mode, int tree, int tag, float *out) {
+  check_use(mode, tree, tag);
+  const TreeWalk *w = nullptr;
+  if ((int)plan_.use_csfs[mode] == tree && (int)plan_.use_tags[mode] == tag) {
+    w = walk_[mode].get();
+  } else {
+    auto &slot = custom_[std::make_tuple(mode, tree, tag)];
+    if (!slot) slot = make_walk(mode, tree, tag);
+    w = slot.get();
+  }
+  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
+  walk_launch(*w, level_factors(tree, opt_.factor_type), opt_.factor_type, out, stream_);
 }
 
 LevelFactors Engine::level_factors(int g, FactorType ft) const {

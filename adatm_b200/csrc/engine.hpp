@@ -2,7 +2,9 @@
 // rows, factor matrices and the CP-ALS sweep.
 #pragma once
 
+#include <map>
 #include <memory>
+#include <tuple>
 #include <vector>
 
 #include "als.cuh"
@@ -71,6 +73,23 @@ class Engine {
   FactorType sweep_type(int mode) const;
   // MTTKRP of `mode` recomputed on its group's tree without memo rows.
   void mttkrp_direct(int mode, float *out);
+  // MTTKRP of `mode` the way a reference caller names it: on tree `tree`
+  // with tag 0 (root MTTKRP; it stores the tree's memo rows when its group
+  // memoizes), 1 (reuse of the tree's memo rows) or 2 (recompute from the
+  // leaves), as mttkrp_csf_adaptive dispatches (mttkrp.c:2037-2090). The
+  // walk is built on first use and kept.
+  void mttkrp_with(int mode, int tree, int tag, float *out);
+  // Whether (mode, tree, tag) is a valid request on this plan's trees:
+  // throws BadInput naming the problem (tag 0 on a mode that is not the
+  // tree's root, tag 2 on the root, tag 1 on a tree without memo rows or
+  // whose memo rows lie above the mode's level).
+  void check_use(int mode, int tree, int tag) const;
+  // Run the sweep with these per-mode trees and tags (a reference caller's
+  // use_csfs / use_tags) instead of the plan's: checked with check_use, and
+  // a tag-1 mode needs the root MTTKRP (tag 0) of its tree at an earlier
+  // mode of the sweep, which writes the memo rows it reads. Rebuilds the
+  // walks and drops a captured sweep when they change.
+  void set_use(const uint64_t *use_csfs, const uint64_t *use_tags);
   float *mttkrp_buffer() { return M_.get(); }
   const float *memo_rows(int g, int deg) const { return memo_[g][deg].get(); }
 
@@ -103,6 +122,7 @@ class Engine {
 
  private:
   void build_walks();
+  std::unique_ptr<TreeWalk> make_walk(int mode, int tree, int tag);
   LevelFactors level_factors(int g, FactorType ft) const;
 
   std::shared_ptr<const DevCoo> coo_;
@@ -115,6 +135,7 @@ class Engine {
   DevBuf<float> memo_[kMaxModes][kMaxModes];
   std::unique_ptr<TreeWalk> walk_[kMaxModes];
   std::unique_ptr<TreeWalk> direct_[kMaxModes];
+  std::map<std::tuple<int, int, int>, std::unique_ptr<TreeWalk>> custom_;  // by (mode, tree, tag)
   DevBuf<float> A_[kMaxModes];
   DevBuf<__nv_bfloat16> Ab_[kMaxModes];
   DevBuf<double> G_[kMaxModes];

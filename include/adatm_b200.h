@@ -178,6 +178,10 @@ typedef struct adatm_candidate {
   uint64_t pops;
 } adatm_candidate;
 
+/* Message of the calling thread's last library call: empty after a call that
+ * succeeded, so the reference's void entry points (mttkrp_csf_adaptive,
+ * bench_adaptm) report failures here too; cpd_als_iterate_adaptive returns
+ * NaN on failure. */
 const char *adatm_last_error(void);
 
 /* Select the CUDA device for the calling thread (the library carries its own
