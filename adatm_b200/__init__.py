@@ -762,6 +762,11 @@ class Engine:
         _check(lib().adatm_engine_set_resident_grid(self._h, int(bool(on))),
                "adatm_engine_set_resident_grid")
 
+    def set_walkers(self, walkers):
+        """Walkers per warp in the contraction source loop (1, 2, 4; 0 =
+        the default for the rank)."""
+        _check(lib().adatm_engine_set_walkers(self._h, int(walkers)), "adatm_engine_set_walkers")
+
 
 class BatchSweep:
     """One ALS iteration of every engine in one CUDA graph; the engines must

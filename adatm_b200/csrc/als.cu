@@ -16,7 +16,6 @@ void AlsWork::init(int nmodes_, int R_, int nblocks_, int max_iters) {
   ldr = ldr_of(R_);
   nblocks = nblocks_;
   vinv64.alloc((size_t)R * R);
-  vinv32.alloc((size_t)R * R);
   part_gram.alloc((size_t)nblocks * R * R);
   part_max.alloc((size_t)nblocks * R);
   part_inner.alloc((size_t)nblocks * R);
@@ -51,13 +50,22 @@ __global__ void k_factor_init(float *A, __nv_bfloat16 *Ab, uint64_t rows, int R,
     const uint64_t x = i * (uint64_t)R + r;
     v = (float)((double)(mix64(key + x) >> 11) * (1.0 / 9007199254740992.0));
   }
+  if (Ab) {
+    // BF16 factors: the rounded value is the factor (see to_bf16)
+    const __nv_bfloat16 b = __float2bfloat16(v);
+    Ab[e] = b;
+    v = __bfloat162float(b);
+  }
   A[e] = v;
-  if (Ab) Ab[e] = __float2bfloat16(v);
 }
 
-__global__ void k_to_bf16(const float *A, __nv_bfloat16 *Ab, uint64_t n) {
+__global__ void k_to_bf16(float *A, __nv_bfloat16 *Ab, uint64_t n) {
   const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e < n) Ab[e] = __float2bfloat16(A[e]);
+  if (e < n) {
+    const __nv_bfloat16 b = __float2bfloat16(A[e]);
+    Ab[e] = b;
+    A[e] = __bfloat162float(b);
+  }
 }
 
 constexpr int kFrobThreads = 256;
@@ -92,7 +100,7 @@ __global__ void k_frob_final(const double *part, int n, double *out) {
 // hence positive). All R steps stay in shared memory.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int mode, int R,
-                                                      double *X, float *X32) {
+                                                      double *X) {
   extern __shared__ double V[];  // R x R, then the pivot column (R)
   double *col = V + R * R;
   const int tid = threadIdx.x;
@@ -123,7 +131,6 @@ __global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int
     const int i = e / R, k = e % R;
     const double v = 0.5 * (V[e] + V[k * R + i]);
     X[e] = v;
-    X32[e] = (float)v;
   }
 }
 
@@ -133,7 +140,7 @@ __global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int
 // ---------------------------------------------------------------------------
 struct UpdArgs {
   const float *M;
-  const float *vinv;  // R x R fp32, or nullptr for identity
+  const double *vinv;  // R x R fp64, or nullptr for identity
   float *A;           // output rows (may alias M when vinv == nullptr)
   uint64_t rows;
   int R, ldr;
@@ -146,9 +153,9 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
   constexpr int GROUPS = 256 / LANES;
   constexpr int RMAX = 4 * LANES;
   constexpr int PAIRS = (RMAX * RMAX + 255) / 256;
-  extern __shared__ float usm[];
-  float *vinv = usm;                      // RMAX x RMAX
-  float *rowbuf = usm + RMAX * RMAX;      // GROUPS x RMAX
+  extern __shared__ double usm[];
+  double *vinv = usm;                                            // RMAX x RMAX
+  float *rowbuf = reinterpret_cast<float *>(usm + RMAX * RMAX);  // GROUPS x RMAX
   const int tid = threadIdx.x;
   const int g = tid / LANES, t = tid % LANES, col = 4 * t;
   const int R = a.R;
@@ -158,7 +165,7 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
   if (a.vinv) {
     for (int e = tid; e < RMAX * RMAX; e += 256) {
       const int k = e / RMAX, c = e % RMAX;
-      vinv[e] = (k < R && c < R) ? a.vinv[k * R + c] : 0.f;
+      vinv[e] = (k < R && c < R) ? a.vinv[k * R + c] : 0.0;
     }
   }
   double gacc[PAIRS];
@@ -175,21 +182,27 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
     if (valid && act) m = *reinterpret_cast<const float4 *>(a.M + i * a.ldr + col);
     float4 o;
     if (a.vinv) {
-      o = make_float4(0.f, 0.f, 0.f, 0.f);
+      // A = M V^-1 with V^-1 and the sums in FP64: V (the Hadamard of the
+      // other modes' Grams) is often ill-conditioned, and FP32 sums of its
+      // inverse's large entries of both signs lose the fit's digits
+      double o0 = 0.0, o1 = 0.0, o2 = 0.0, o3 = 0.0;
       for (int kk = 0; kk < kq; ++kk) {
-        const float m0 = __shfl_sync(gmask, m.x, kk, LANES);
-        const float m1 = __shfl_sync(gmask, m.y, kk, LANES);
-        const float m2 = __shfl_sync(gmask, m.z, kk, LANES);
-        const float m3 = __shfl_sync(gmask, m.w, kk, LANES);
-        const float4 v0 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 0) * RMAX + col);
-        const float4 v1 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 1) * RMAX + col);
-        const float4 v2 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 2) * RMAX + col);
-        const float4 v3 = *reinterpret_cast<const float4 *>(vinv + (4 * kk + 3) * RMAX + col);
-        o.x = fmaf(m0, v0.x, fmaf(m1, v1.x, fmaf(m2, v2.x, fmaf(m3, v3.x, o.x))));
-        o.y = fmaf(m0, v0.y, fmaf(m1, v1.y, fmaf(m2, v2.y, fmaf(m3, v3.y, o.y))));
-        o.z = fmaf(m0, v0.z, fmaf(m1, v1.z, fmaf(m2, v2.z, fmaf(m3, v3.z, o.z))));
-        o.w = fmaf(m0, v0.w, fmaf(m1, v1.w, fmaf(m2, v2.w, fmaf(m3, v3.w, o.w))));
+        const double m4[4] = {(double)__shfl_sync(gmask, m.x, kk, LANES),
+                              (double)__shfl_sync(gmask, m.y, kk, LANES),
+                              (double)__shfl_sync(gmask, m.z, kk, LANES),
+                              (double)__shfl_sync(gmask, m.w, kk, LANES)};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const double *vr = vinv + (4 * kk + q) * RMAX + col;
+          const double2 lo = *reinterpret_cast<const double2 *>(vr);
+          const double2 hi = *reinterpret_cast<const double2 *>(vr + 2);
+          o0 = fma(m4[q], lo.x, o0);
+          o1 = fma(m4[q], lo.y, o1);
+          o2 = fma(m4[q], hi.x, o2);
+          o3 = fma(m4[q], hi.y, o3);
+        }
       }
+      o = make_float4((float)o0, (float)o1, (float)o2, (float)o3);
       if (valid && act) *reinterpret_cast<float4 *>(a.A + i * a.ldr + col) = o;
     } else {
       o = m;
@@ -299,15 +312,19 @@ __global__ void __launch_bounds__(256) k_scale(float *A, __nv_bfloat16 *Ab, cons
     v.y *= il.y;
     v.z *= il.z;
     v.w *= il.w;
-    *reinterpret_cast<float4 *>(A + i * ldr + col) = v;
     if (Ab) {
+      // BF16 factors: the rounded row replaces the FP32 row too, so the
+      // Gram, the MTTKRPs and the fit all see the same factor
       __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y);
       __nv_bfloat162 hi = __floats2bfloat162_rn(v.z, v.w);
       uint2 raw;
       raw.x = *reinterpret_cast<uint32_t *>(&lo);
       raw.y = *reinterpret_cast<uint32_t *>(&hi);
       *reinterpret_cast<uint2 *>(Ab + i * ldr + col) = raw;
+      const float2 flo = __bfloat1622float2(lo), fhi = __bfloat1622float2(hi);
+      v = make_float4(flo.x, flo.y, fhi.x, fhi.y);
     }
+    *reinterpret_cast<float4 *>(A + i * ldr + col) = v;
     if (part_inner) {
       const float4 m = *reinterpret_cast<const float4 *>(M + i * ldr + col);
       in0 += (double)v.x * m.x;
@@ -389,7 +406,8 @@ int lanes_for(int R) {
 
 template <int LANES>
 constexpr size_t update_smem() {
-  return (size_t)(4 * LANES * 4 * LANES + (256 / LANES) * 4 * LANES) * sizeof(float);
+  return (size_t)(4 * LANES * 4 * LANES) * sizeof(double) +
+         (size_t)((256 / LANES) * 4 * LANES) * sizeof(float);
 }
 
 template <int LANES>
@@ -447,7 +465,7 @@ void factor_init_device(float *A, __nv_bfloat16 *Ab, uint64_t rows, int R, int l
   ADATM_LAUNCH();
 }
 
-void to_bf16(const float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s) {
+void to_bf16(float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s) {
   const uint64_t n = rows * (uint64_t)ldr;
   if (n == 0) return;
   k_to_bf16<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, Ab, n);
@@ -483,7 +501,7 @@ void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s) {
 
 void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s) {
   const size_t smem = (size_t)(w.R * w.R + w.R) * sizeof(double);
-  k_gram_inverse<<<1, 256, smem, s>>>(g, w.nmodes, mode, w.R, w.vinv64.get(), w.vinv32.get());
+  k_gram_inverse<<<1, 256, smem, s>>>(g, w.nmodes, mode, w.R, w.vinv64.get());
   ADATM_LAUNCH();
 }
 
@@ -491,7 +509,7 @@ void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, d
                    bool inner, AlsWork &w, cudaStream_t s) {
   UpdArgs u;
   u.M = M;
-  u.vinv = w.vinv32.get();
+  u.vinv = w.vinv64.get();
   u.A = A;
   u.rows = rows;
   u.R = w.R;
@@ -511,6 +529,10 @@ void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, d
     default: k_scale<32><<<w.nblocks, 256, 0, s>>>(A, Ab, M, rows, w.R, w.ldr, w.lambda.get(), pi); break;
   }
   ADATM_LAUNCH();
+  // BF16 factors were rounded after the Gram was taken: take it again from
+  // the rounded rows, so the next modes' normal equations use the factor the
+  // MTTKRPs read
+  if (Ab) gram(A, rows, w.R, w.ldr, G_mode, w, s);
 }
 
 void fit(const GramSet &g, AlsWork &w, cudaStream_t s) {

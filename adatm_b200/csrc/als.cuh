@@ -12,7 +12,6 @@ struct AlsWork {
   int nmodes = 0, R = 0, ldr = 0;
   int nblocks = 0;                       // row blocks of the update kernels
   DevBuf<double> vinv64;                 // R x R
-  DevBuf<float> vinv32;                  // R x R
   DevBuf<double> part_gram;              // nblocks x R x R
   DevBuf<double> part_max;               // nblocks x R
   DevBuf<double> part_inner;             // nblocks x R
@@ -37,12 +36,13 @@ void factor_init_device(float *A, __nv_bfloat16 *Ab, uint64_t rows, int R, int l
 void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, cudaStream_t s);
 // sum of squares of the tensor values -> w.scalars[0]
 void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s);
-// V = Hadamard of all G[n], n != mode; write V^-1 (fp32 and fp64) via Cholesky.
+// V = Hadamard of all G[n], n != mode; write V^-1 (fp64).
 void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s);
 // A = normalize(M * V^-1); updates lambda (2-norm on the first iteration,
 // max-norm floored at 1 afterwards), G_mode and, when `inner` is set, the
-// partial inner products <A, M> of the fit. A is fp32 with a bf16 copy (Ab,
-// may be null).
+// partial inner products <A, M> of the fit. A is fp32; with a bf16 copy (Ab
+// non-null) the rows are rounded to bf16 in both copies and G_mode is taken
+// from the rounded rows.
 void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
                    bool inner, AlsWork &w, cudaStream_t s);
 // fit = 1 - sqrt(||X||^2 + ||Z||^2 - 2<X,Z>) / ||X||, stored in
@@ -53,7 +53,8 @@ void fit(const GramSet &g, AlsWork &w, cudaStream_t s);
 // calls that overlap in time on one device race on the shared array.
 void gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, cudaStream_t s);
 int gram_noalloc_max_rank();
-// Convert fp32 rows to bf16 (rows x ldr).
-void to_bf16(const float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s);
+// Round fp32 rows to bf16 (rows x ldr) into Ab and write the rounded values
+// back to A: with BF16 factors the rounded value is the factor everywhere.
+void to_bf16(float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s);
 
 }  // namespace adatm

@@ -1238,6 +1238,14 @@ int adatm_engine_set_resident_grid(adatm_engine *e, int on) {
   });
 }
 
+int adatm_engine_set_walkers(adatm_engine *e, int walkers) {
+  return guarded([&] {
+    if (!e) throw BadInput("adatm_engine_set_walkers: null engine");
+    e->eng->set_walkers(walkers);
+    e->graph = false;
+  });
+}
+
 int adatm_batch_create(adatm_engine *const *engines, int n, adatm_batch **out) {
   return guarded([&] {
     if (n < 1 || !engines || !out) throw BadInput("adatm_batch_create: no engines");

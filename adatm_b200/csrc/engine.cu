@@ -166,6 +166,19 @@ void Engine::set_chunks(uint32_t chunk_leaf, uint32_t chunk_rows) {
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
+void Engine::set_walkers(int walkers) {
+  if (walkers != 0 && !walkers_supported((int)R_, walkers))
+    throw BadInput("no contraction kernel for " + std::to_string(walkers) + " walkers at rank " +
+                   std::to_string(R_));
+  drop_graph();
+  opt_.walkers = walkers;
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    walk_[m]->walkers = walkers;
+    direct_[m]->walkers = walkers;
+  }
+  for (auto &kv : custom_) kv.second->walkers = walkers;
+}
+
 void Engine::set_resident_grid(bool on) {
   drop_graph();
   opt_.resident_grid = on;
@@ -361,6 +374,7 @@ std::unique_ptr<TreeWalk> Engine::make_walk(int mode, int g, int tag) {
   w->out = d;
   w->chunk = opt_.chunk_leaf;
   w->resident = opt_.resident_grid;
+  w->walkers = opt_.walkers;
   if (tag == 0 && gp.n_imten > 0) {
     // memo root: store level begin_imten-1-deg into memo tree deg
     for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
@@ -443,15 +457,12 @@ void Engine::mttkrp_as(int mode, float *out, FactorType ft) {
 void Engine::mttkrp(int mode, float *out) { mttkrp_as(mode, out, opt_.factor_type); }
 
 FactorType Engine::sweep_type(int mode) const {
-  // The last mode's MTTKRP M also gives <X, Z> for the fit. An error E in M
-  // moves the computed residual by -2<E, M V^-1>, a positive-definite term
-  // that BF16 gathers make as large as the residual itself (the fit then
-  // overshoots, or its square root goes negative). So every MTTKRP of the
-  // tree that feeds the last mode -- its own walk and the memo rows it
-  // reuses -- reads FP32 rows.
-  const int N = coo_->nmodes;
-  if (opt_.factor_type == FactorType::F32) return FactorType::F32;
-  return plan_.use_csfs[mode] == plan_.use_csfs[N - 1] ? FactorType::F32 : opt_.factor_type;
+  // With BF16 factors every factor value is BF16-representable (the update
+  // rounds both copies, and the Grams are taken from the rounded rows), so
+  // every walk gathers the half-width rows and sees exactly the factor the
+  // normal equations and the fit use.
+  (void)mode;
+  return opt_.factor_type;
 }
 
 void Engine::mttkrp_direct(int mode, float *out) {
@@ -468,7 +479,10 @@ int Engine::kernels_per_mttkrp(int mode) const {
 
 int Engine::kernels_per_sweep() const {
   int k = 1;  // fit
-  for (int m = 0; m < coo_->nmodes; ++m) k += kernels_per_mttkrp(m) + 4;
+  // per mode: the walks, the Gram inverse, the update, its finalize, the
+  // scale; BF16 factors add the Gram of the rounded rows (two kernels)
+  const int dense = opt_.factor_type == FactorType::BF16 ? 6 : 4;
+  for (int m = 0; m < coo_->nmodes; ++m) k += kernels_per_mttkrp(m) + dense;
   return k;
 }
 

@@ -22,6 +22,8 @@ struct EngineOptions {
   // for one tensor on the device); off, one chunk per warp, so the blocks of
   // walks running side by side on other streams interleave
   bool resident_grid = true;
+  // walkers per warp in the contraction source loop (0 = default_walkers(R))
+  int walkers = 0;
 };
 
 class Engine {
@@ -111,6 +113,9 @@ class Engine {
   // Contraction grid shape (EngineOptions::resident_grid); drops a captured
   // sweep.
   void set_resident_grid(bool on);
+  // Walkers per warp of the contraction walks (1, 2, 4; 0 = the default
+  // for the rank); drops a captured sweep.
+  void set_walkers(int walkers);
   uint32_t chunk_leaf() const { return opt_.chunk_leaf; }
   uint32_t chunk_rows() const { return opt_.chunk_rows; }
   // Time `count` graph-replayed sweeps (CUDA events, ms total).

@@ -240,8 +240,12 @@ struct RowSrc {
 // (and parent) words and a 32-word exchange buffer.
 template <int V>
 __host__ __device__ constexpr size_t contract_warp_smem(int N) {
-  return (size_t)(kBatch + N - 1) * 32 * sizeof(fv<V>) + kBatch * (sizeof(uint4) + sizeof(uint32_t));
+  return (size_t)(kBatch + N - 1) * 32 * sizeof(fv<V>) +
+         (kBatch + kBatch / 16) * sizeof(uint4) + kBatch * sizeof(uint32_t);
 }
+// Staging slot of batch unit k: one spare uint4 every 16 units, so the two
+// or four walkers of a warp reading units 16 apart hit different banks.
+__device__ __forceinline__ int ustage_slot(int k) { return k + (k >> 4); }
 template <int V>
 constexpr size_t contract_smem(int N) {
   return (size_t)kWarps * contract_warp_smem<V>(N);
@@ -301,19 +305,37 @@ constexpr int contract_min_blocks() {
 // row (U_{S-1} of the level-(S-1) node holding it) and summed straight into
 // the open node of level S-2, so the batch's items are level-(S-2) nodes.
 // The sums equal the unfused ones up to FP32 rounding order.
-template <int V, FactorType FT, bool LEAF, bool FUSE>
+// WALKERS: the source loop of a batch runs as W walkers of 32/W lanes, each
+// over its own contiguous segment of 32/W units with VW columns per lane, so
+// one warp instruction advances W units. Each walker sums its segment into
+// its own open node; the nodes that close in a walker's segment become items
+// as before, and the segments are joined once per batch: the sum a walker
+// carries past its segment flows into the next walker's first closed node
+// (or on through, when that walker closes none), W - 1 shuffle rounds. The
+// level loop keeps the warp-wide layout (V columns per lane); items and
+// carry rows are plain column-ordered rows in shared memory, so both
+// layouts read them.
+template <int V, int W, int VW, FactorType FT, bool LEAF, bool FUSE>
 __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     k_contract(const __grid_constant__ WalkArgs a) {
+  static_assert(W == 1 || W == 2 || W == 4, "walkers per warp");
+  static_assert((32 / W) * VW <= 32 * V, "a walker's columns must fit the item rows");
+  constexpr int L = 32 / W;        // lanes per walker
+  constexpr int SEG = kBatch / W;  // units per walker per batch
   extern __shared__ __align__(16) unsigned char walk_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char *wbase = walk_raw + (size_t)warp * contract_warp_smem<V>(a.N);
   fv<V> *items = reinterpret_cast<fv<V> *>(wbase);
+  float *items_f = reinterpret_cast<float *>(wbase);  // row j: 32 * V floats
   fv<V> *carry = items + kBatch * 32;  // rows d..S-1
   fv<V> *pre = carry;                  // rows 0..d-1
   uint4 *ustage = reinterpret_cast<uint4 *>(carry + (a.N - 1) * 32);
-  uint32_t *xbuf = reinterpret_cast<uint32_t *>(ustage + kBatch);
+  uint32_t *xbuf = reinterpret_cast<uint32_t *>(ustage + kBatch + kBatch / 16);
   const int col = lane * V;
   const bool act = col < a.R;
+  const int wk = lane / L;           // this lane's walker
+  const int wcol = (lane % L) * VW;  // its first column in the walker layout
+  const bool wact = wcol < a.R;
   const int S = a.S, d = a.d;
   // a resident grid: each warp claims chunks from a counter, the next one
   // while it walks the current one; without a counter, one chunk per warp
@@ -328,11 +350,13 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     uint32_t touched = 0;
     for (int l = d; l < S - 1; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
     if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
-    const RowSrc<V, FT> Us(a.U_src, a.ldr, col, act);
-    const RowSrc<V, FT> Up(FUSE ? a.U[S - 1] : a.U_src, a.ldr, col, act);
+    const RowSrc<VW, FT> Us(a.U_src, a.ldr, wcol, wact);
+    const RowSrc<VW, FT> Up(FUSE ? a.U[S - 1] : a.U_src, a.ldr, wcol, wact);
     const int top = FUSE ? S - 2 : S - 1;  // level whose open node the units feed
-    fv<V> acc = fv_fill<V>(0.f);           // open node of level `top`
-    constexpr int SB = (FUSE ? 8 : 16) / V;  // unit rows in flight per lane
+    // open node of level `top` carried in from earlier batches (every walker
+    // holds the same copy)
+    fv<VW> acc = fv_fill<VW>(0.f);
+    constexpr int SB = (FUSE ? 8 : 16) / VW;  // unit rows in flight per lane
     const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
     const uint64_t u1 = min(u0 + a.chunk, a.nunits);
     for (uint64_t base = u0; base < u1; base += kBatch) {
@@ -350,46 +374,56 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
         if (in && pn < a.nfibs[S - 1]) pfid = __ldg(a.fids[S - 1] + pn);
       }
       const uint32_t Mc = FUSE ? __ballot_sync(~0u, cd >= 2u) : M;  // closes of level `top`
-      ustage[lane] = make_uint4(id, __float_as_uint(v), pfid, 0u);
+      ustage[ustage_slot(lane)] = make_uint4(id, __float_as_uint(v), pfid, 0u);
       __syncwarp();
-      int j = 0;
+      // this walker's units are k_lo .. k_lo + SEG - 1: its closes, and the
+      // item index of its first close
+      const int k_lo = wk * SEG;
+      const uint32_t below = k_lo == 0 ? 0u : (0xFFFFFFFFu >> (32 - k_lo));
+      const uint32_t Mw = Mc & ((0xFFFFFFFFu >> (32 - SEG)) << k_lo);
+      const int j0 = __popc(Mc & below);
+      int j = j0;
+      fv<VW> wacc = W == 1 ? acc : fv_fill<VW>(0.f);
+      auto emit = [&](const fv<VW> &x) {
+        *reinterpret_cast<fv<VW> *>(items_f + (size_t)j * 32 * V + wcol) = x;
+        ++j;
+      };
       auto run = [&](auto full) {
         constexpr bool FULL = decltype(full)::value;
 #pragma unroll
-        for (int k0 = 0; k0 < kBatch; k0 += SB) {
-          if (!FULL && k0 >= cnt) break;
-          fv<V> g[SB];
-          fv<V> h[FUSE ? SB : 1];
-          fv<V> m[LEAF ? 1 : SB];
+        for (int q0 = 0; q0 < SEG; q0 += SB) {
+          if (!FULL && k_lo + q0 >= cnt) break;
+          fv<VW> g[SB];
+          fv<VW> h[FUSE ? SB : 1];
+          fv<VW> m[LEAF ? 1 : SB];
           float vv[LEAF ? SB : 1];
 #pragma unroll
           for (int q = 0; q < SB; ++q) {
-            const int k = k0 + q;
+            const int k = k_lo + q0 + q;
             // lanes past the rank read column 0 through Us's base, so only
             // the units past the batch need the row-0 substitute
             const bool ok = FULL || k < cnt;
-            const uint4 e = ustage[k];
+            const uint4 e = ustage[ustage_slot(k)];
             g[q] = Us.load(e.x, ok);
             if constexpr (FUSE) h[q] = Up.load(e.z, ok);
             if constexpr (LEAF) vv[q] = __uint_as_float(e.y);
-            if constexpr (!LEAF) m[q] = ld_rows<V>(a.src_rows, base + k, a.ldr, col, ok && act);
+            if constexpr (!LEAF) m[q] = ld_rows<VW>(a.src_rows, base + k, a.ldr, wcol, ok && wact);
           }
 #pragma unroll
           for (int q = 0; q < SB; ++q) {
-            const int k = k0 + q;
+            const int k = k_lo + q0 + q;
             if (FULL || k < cnt) {
               if constexpr (FUSE) {
-                const fv<V> x = LEAF ? fv_scale(vv[LEAF ? q : 0], g[q]) : fv_mul(m[LEAF ? 0 : q], g[q]);
-                fv_fma(acc, x, h[FUSE ? q : 0]);
+                const fv<VW> x = LEAF ? fv_scale(vv[LEAF ? q : 0], g[q]) : fv_mul(m[LEAF ? 0 : q], g[q]);
+                fv_fma(wacc, x, h[FUSE ? q : 0]);
               } else if constexpr (LEAF) {
-                fv_axpy(acc, vv[LEAF ? q : 0], g[q]);
+                fv_axpy(wacc, vv[LEAF ? q : 0], g[q]);
               } else {
-                fv_fma(acc, m[LEAF ? 0 : q], g[q]);
+                fv_fma(wacc, m[LEAF ? 0 : q], g[q]);
               }
-              if ((Mc >> k) & 1u) {
-                items[j * 32 + lane] = acc;
-                acc = fv_fill<V>(0.f);
-                ++j;
+              if ((Mw >> k) & 1u) {
+                emit(wacc);
+                wacc = fv_fill<VW>(0.f);
               }
             }
           }
@@ -397,6 +431,37 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       };
       if (cnt == kBatch) run(std::true_type{});
       else run(std::false_type{});
+      if constexpr (W == 1) {
+        acc = wacc;
+      } else {
+        // join the segments: the inflow of walker w is what walker w-1
+        // carries past its segment (the carry-in for walker 0)
+        const bool hc = Mw != 0u;
+        fv<VW> inflow = acc, out;
+#pragma unroll
+        for (int i = 0; i < VW; ++i) out.x[i] = hc ? wacc.x[i] : inflow.x[i] + wacc.x[i];
+#pragma unroll
+        for (int r = 0; r + 1 < W; ++r) {
+#pragma unroll
+          for (int i = 0; i < VW; ++i) {
+            const float up = __shfl_up_sync(~0u, out.x[i], L);
+            if (wk == r + 1) {
+              inflow.x[i] = up;
+              out.x[i] = hc ? wacc.x[i] : up + wacc.x[i];
+            }
+          }
+        }
+        if (hc) {
+          fv<VW> *first = reinterpret_cast<fv<VW> *>(items_f + (size_t)j0 * 32 * V + wcol);
+          fv<VW> t = *first;
+#pragma unroll
+          for (int i = 0; i < VW; ++i) t.x[i] += inflow.x[i];
+          *first = t;
+        }
+#pragma unroll
+        for (int i = 0; i < VW; ++i) acc.x[i] = __shfl_sync(~0u, out.x[i], (W - 1) * L + lane % L);
+      }
+      __syncwarp();
       if ((Mc >> (cnt - 1)) & 1u) touched &= ~(1u << top);
       else touched |= 1u << top;
       if (FUSE && M != 0u) {
@@ -463,7 +528,10 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       }
     }
     // chunk end: the open nodes of levels top .. d add their partial sums
-    carry[top * 32 + lane] = acc;
+    // (the carried row, in the walker layout, is written by walker 0)
+    if (wk == 0)
+      *reinterpret_cast<fv<VW> *>(reinterpret_cast<float *>(carry) + (size_t)top * 32 * V + wcol) = acc;
+    __syncwarp();
     for (int l = top; l >= d; --l) {
       if (!((touched >> l) & 1u)) continue;
       const uint32_t node = __shfl_sync(~0u, nodeL, l);
@@ -785,17 +853,18 @@ unsigned resident_blocks(K kernel, int threads, size_t smem) {
   return (unsigned)std::max(1, sms * std::max(1, per_sm));
 }
 
-template <int V, FactorType FT, bool LEAF, bool FUSE>
+template <int V, int W, int VW, FactorType FT, bool LEAF, bool FUSE>
 void launch_contract_v(const WalkArgs &a, unsigned blocks, bool resident, cudaStream_t s) {
   const size_t smem = contract_smem<V>(a.N);
+  auto kern = k_contract<V, W, VW, FT, LEAF, FUSE>;
   if (resident) {
-    blocks = std::min(blocks, resident_blocks(k_contract<V, FT, LEAF, FUSE>, 256, smem));
+    blocks = std::min(blocks, resident_blocks(kern, 256, smem));
     ADATM_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), s));
-    k_contract<V, FT, LEAF, FUSE><<<blocks, 256, smem, s>>>(a);
+    kern<<<blocks, 256, smem, s>>>(a);
   } else {
     WalkArgs b = a;
     b.counter = nullptr;  // one chunk per warp: blocks cover every chunk
-    k_contract<V, FT, LEAF, FUSE><<<blocks, 256, smem, s>>>(b);
+    kern<<<blocks, 256, smem, s>>>(b);
   }
 }
 
@@ -803,25 +872,36 @@ void launch_contract_v(const WalkArgs &a, unsigned blocks, bool resident, cudaSt
 // the output level.
 bool fusable(const WalkArgs &a) { return a.S - 1 > a.d && a.store[a.S - 1] == nullptr; }
 
+// The (V, W, VW) shapes the contraction is built for: V columns per lane in
+// the level loop (32 lanes cover the rank), W walkers in the source loop
+// with VW columns per lane (32 / W lanes cover the rank).
+#define ADATM_CONTRACT_SHAPES(X) \
+  X(1, 1, 1) X(1, 2, 1) X(1, 2, 2) X(1, 4, 1) X(1, 4, 2) X(1, 4, 4) X(2, 1, 2) X(2, 2, 4) X(4, 1, 4)
+
+// Columns per walker lane for W walkers at rank R (0 if W walkers cannot
+// cover R with at most 4 columns per lane).
+int walker_cols(int R, int W) {
+  for (int vw : {1, 2, 4})
+    if ((32 / W) * vw >= R) return vw;
+  return 0;
+}
+
 template <FactorType FT, bool LEAF>
-void launch_contract(int vec, const WalkArgs &a, unsigned blocks, bool resident, cudaStream_t s) {
+void launch_contract(int vec, int walkers, const WalkArgs &a, unsigned blocks, bool resident,
+                     cudaStream_t s) {
   const bool fuse = fusable(a);
-  switch (vec) {
-    case 1:
-      if (fuse) launch_contract_v<1, FT, LEAF, true>(a, blocks, resident, s);
-      else launch_contract_v<1, FT, LEAF, false>(a, blocks, resident, s);
-      break;
-    case 2:
-      if (fuse) launch_contract_v<2, FT, LEAF, true>(a, blocks, resident, s);
-      else launch_contract_v<2, FT, LEAF, false>(a, blocks, resident, s);
-      break;
-    case 4:
-      if (fuse) launch_contract_v<4, FT, LEAF, true>(a, blocks, resident, s);
-      else launch_contract_v<4, FT, LEAF, false>(a, blocks, resident, s);
-      break;
-    default: throw BadInput("unsupported columns per lane");
+  const int vw = walker_cols(a.R, walkers);
+#define ADATM_CONTRACT_CASE(V, W, VW)                                              \
+  if (vec == V && walkers == W && vw == VW) {                                      \
+    if (fuse) launch_contract_v<V, W, VW, FT, LEAF, true>(a, blocks, resident, s); \
+    else launch_contract_v<V, W, VW, FT, LEAF, false>(a, blocks, resident, s);     \
+    ADATM_LAUNCH();                                                                \
+    return;                                                                        \
   }
-  ADATM_LAUNCH();
+  ADATM_CONTRACT_SHAPES(ADATM_CONTRACT_CASE)
+#undef ADATM_CONTRACT_CASE
+  throw BadInput("no contraction kernel for " + std::to_string(walkers) + " walkers at rank " +
+                 std::to_string(a.R));
 }
 
 template <int W, FactorType FT, bool LEAF>
@@ -856,6 +936,24 @@ int vec_for_rank(int R) {
   throw BadInput("rank above 128 is not supported by the GPU kernels");
 }
 
+}  // namespace
+
+int default_walkers(int R) { return R <= 64 ? 2 : 1; }
+
+bool walkers_supported(int R, int W) {
+  if (W != 1 && W != 2 && W != 4) return false;
+  const int v = R <= 32 ? 1 : (R <= 64 ? 2 : 4);
+  const int vw = walker_cols(R, W);
+  if (vw == 0) return false;
+#define ADATM_CONTRACT_OK(V, WW, VW) \
+  if (v == V && W == WW && vw == VW) return true;
+  ADATM_CONTRACT_SHAPES(ADATM_CONTRACT_OK)
+#undef ADATM_CONTRACT_OK
+  return false;
+}
+
+namespace {
+
 // Scatter: lanes per unit (4 columns per lane).
 int lanes_for_rank(int R) {
   if (R <= 16) return 4;
@@ -870,13 +968,18 @@ int lanes_for_rank(int R) {
 void set_walk_attributes() {
   static bool done = false;
   if (done) return;
-#define ADATM_ATTR_C(V, FT, LEAF)                                                 \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, false>,                 \
+#define ADATM_ATTR_C1(V, W, VW, FT, LEAF)                                         \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, W, VW, FT, LEAF, false>,          \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)contract_smem<V>(kMaxModes)));             \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, FT, LEAF, true>,                  \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, W, VW, FT, LEAF, true>,           \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)contract_smem<V>(kMaxModes)));
+#define ADATM_ATTR_CS(V, W, VW)                       \
+  ADATM_ATTR_C1(V, W, VW, FactorType::F32, true)      \
+  ADATM_ATTR_C1(V, W, VW, FactorType::F32, false)     \
+  ADATM_ATTR_C1(V, W, VW, FactorType::BF16, true)     \
+  ADATM_ATTR_C1(V, W, VW, FactorType::BF16, false)
 #define ADATM_ATTR_S(W, FT, LEAF)                                                 \
   ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF, false>,                  \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
@@ -890,16 +993,15 @@ void set_walk_attributes() {
   M(X, FactorType::F32, false)              \
   M(X, FactorType::BF16, true)              \
   M(X, FactorType::BF16, false)
-  ADATM_ATTR_ALL(ADATM_ATTR_C, 1)
-  ADATM_ATTR_ALL(ADATM_ATTR_C, 2)
-  ADATM_ATTR_ALL(ADATM_ATTR_C, 4)
+  ADATM_CONTRACT_SHAPES(ADATM_ATTR_CS)
   ADATM_ATTR_ALL(ADATM_ATTR_S, 4)
   ADATM_ATTR_ALL(ADATM_ATTR_S, 8)
   ADATM_ATTR_ALL(ADATM_ATTR_S, 16)
   ADATM_ATTR_ALL(ADATM_ATTR_S, 32)
 #undef ADATM_ATTR_ALL
 #undef ADATM_ATTR_S
-#undef ADATM_ATTR_C
+#undef ADATM_ATTR_CS
+#undef ADATM_ATTR_C1
   done = true;
 }
 
@@ -971,12 +1073,13 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
   const bool leaf = w.src == w.nmodes - 1;
   if (w.src > w.out) {
     const int vec = vec_for_rank(w.R);
+    const int wk = w.walkers > 0 ? w.walkers : default_walkers(w.R);
     if (ft == FactorType::F32) {
-      if (leaf) launch_contract<FactorType::F32, true>(vec, a, blocks, w.resident, s);
-      else launch_contract<FactorType::F32, false>(vec, a, blocks, w.resident, s);
+      if (leaf) launch_contract<FactorType::F32, true>(vec, wk, a, blocks, w.resident, s);
+      else launch_contract<FactorType::F32, false>(vec, wk, a, blocks, w.resident, s);
     } else {
-      if (leaf) launch_contract<FactorType::BF16, true>(vec, a, blocks, w.resident, s);
-      else launch_contract<FactorType::BF16, false>(vec, a, blocks, w.resident, s);
+      if (leaf) launch_contract<FactorType::BF16, true>(vec, wk, a, blocks, w.resident, s);
+      else launch_contract<FactorType::BF16, false>(vec, wk, a, blocks, w.resident, s);
     }
   } else {
     const int lanes = lanes_for_rank(w.R);

@@ -49,6 +49,8 @@ struct TreeWalk {
   DevBuf<uint32_t> sched;                    // nchunks x (S + 1), then the chunk counter
   bool resident = true;                      // contraction grid: resident blocks that claim
                                              // chunks (else one chunk per warp)
+  int walkers = 0;                           // contraction source loop: walkers per warp
+                                             // (1, 2 or 4; 0 = default_walkers(R))
   // Scatter walks: the output rows that the most units hit (at most
   // kHotRows, each hit by at least kHotMin units) are summed per block in
   // shared memory; hot_slot maps an output row to its slot (0xFF = none).
@@ -61,6 +63,11 @@ struct TreeWalk {
     return false;
   }
 };
+
+// Walkers per warp of the contraction's source loop by default at rank R,
+// and whether W walkers are built for rank R.
+int default_walkers(int R);
+bool walkers_supported(int R, int W);
 
 // Fill the chunk schedule: node ids at levels 0..S-1 of every chunk's first
 // unit, plus a bit mask of the levels whose node began before the chunk.

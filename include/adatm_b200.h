@@ -279,6 +279,14 @@ int adatm_engine_autotune(adatm_engine *e, const uint32_t *chunk_leaf, const uin
  * Drops a captured sweep. No reference counterpart (a launch-shape control). */
 int adatm_engine_set_resident_grid(adatm_engine *e, int on);
 
+/* Walkers per warp in the contraction walks' source loop: 1, 2 or 4 (0 =
+ * the default for the rank). With W walkers one warp instruction advances W
+ * source units (32/W lanes and up to 4 columns per lane each); refused with
+ * SPLATT_ERROR_BADINPUT where W walkers cannot cover the rank. Results agree
+ * up to FP32 summation order. Drops a captured sweep. No reference
+ * counterpart (a launch-shape control). */
+int adatm_engine_set_walkers(adatm_engine *e, int walkers);
+
 /* One ALS iteration of every engine in one CUDA graph (each engine on its
  * own branch). The engines must outlive the batch. */
 typedef struct adatm_batch adatm_batch;

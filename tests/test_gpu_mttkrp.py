@@ -164,3 +164,36 @@ def test_analytic_plan_matches_oracle(gpu):
         assert plan["groups"] == d["groups"], name
         _, ocfg = O.plan(d["inds"], d["dims_list"], int(d["R"]))
         assert [(c["pspace"], c["pops"]) for c in cands] == [(c["pspace"], c["pops"]) for c in ocfg]
+
+
+@pytest.mark.parametrize("R", [5, 16, 32, 48, 64, 100])
+@pytest.mark.parametrize("walkers", [1, 2, 4])
+def test_walker_split(gpu, R, walkers):
+    """The contraction source loop split into 1, 2 or 4 walkers per warp
+    (segments joined once per batch) gives the oracle's MTTKRP sequence on
+    every plan kind, with chunks that cut nodes at every level; walker counts
+    that cannot cover the rank are refused."""
+    A = gpu
+    inds, vals, dims = draw_coo([40, 30, 25, 20, 12], 30000, 17, 1.3)
+    ci, cv, cd = O.coo_clean(inds, vals, dims)
+    cd = [int(x) for x in cd]
+    t = A.Tensor.from_coo(ci, cv, cd)
+    _, cands, _ = A.plan_analytic(t, R)
+    mats = O.init_factors(cd, R, 3)
+    ok = {(1, 1): R <= 128, (1, 2): R <= 64, (1, 4): R <= 32}[(1, walkers)]
+    for c in cands[:3]:
+        for chunk in (0, 7):
+            e = A.Engine(t, R, c, chunk_leaf=chunk, chunk_rows=chunk)
+            if not ok:
+                with pytest.raises(A.AdatmError):
+                    e.set_walkers(walkers)
+                e.free()
+                return
+            e.set_walkers(walkers)
+            e.set_factors(mats)
+            om = O.Model(ci, cv, cd, R, c["groups"])
+            for m in range(5):
+                want = om.mttkrp(mats, m)
+                assert rel_err(e.mttkrp(m), want) < TOL_F32, (m, chunk)
+                assert rel_err(e.mttkrp_direct(m), want) < TOL_F32, (m, chunk)
+            e.free()
