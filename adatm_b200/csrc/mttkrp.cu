@@ -356,7 +356,9 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     // open node of level `top` carried in from earlier batches (every walker
     // holds the same copy)
     fv<VW> acc = fv_fill<VW>(0.f);
-    constexpr int SB = (FUSE ? 8 : 16) / VW;  // unit rows in flight per lane
+    // unit rows in flight per lane, never more than the walker's segment
+    constexpr int SB = ((FUSE ? 8 : 16) / VW) < SEG ? ((FUSE ? 8 : 16) / VW) : SEG;
+    static_assert(SEG % SB == 0, "a walker's segment is a whole number of load groups");
     const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
     const uint64_t u1 = min(u0 + a.chunk, a.nunits);
     for (uint64_t base = u0; base < u1; base += kBatch) {

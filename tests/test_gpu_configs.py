@@ -101,8 +101,7 @@ def test_mttkrp_each_mode_full_size(gpu, name, bf16):
     e.free()
 
 
-@pytest.mark.parametrize("name", list(CONFIGS))
-@pytest.mark.parametrize("bf16", [False, True])
+@pytest.mark.parametrize("name,bf16", [(n, False) for n in CONFIGS] + [("bf16_5mode", True)])
 def test_fit_after_full_sweeps(gpu, name, bf16):
     A = gpu
     t, inds, vals, dims, plan = workload(A, name)
