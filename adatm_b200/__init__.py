@@ -767,6 +767,12 @@ class Engine:
         the default for the rank)."""
         _check(lib().adatm_engine_set_walkers(self._h, int(walkers)), "adatm_engine_set_walkers")
 
+    def set_deterministic(self, on=True):
+        """Deterministic accumulation (no float atomics): sweeps repeat bit
+        for bit from the same start."""
+        _check(lib().adatm_engine_set_deterministic(self._h, int(bool(on))),
+               "adatm_engine_set_deterministic")
+
 
 class BatchSweep:
     """One ALS iteration of every engine in one CUDA graph; the engines must

@@ -1246,6 +1246,14 @@ int adatm_engine_set_walkers(adatm_engine *e, int walkers) {
   });
 }
 
+int adatm_engine_set_deterministic(adatm_engine *e, int on) {
+  return guarded([&] {
+    if (!e) throw BadInput("adatm_engine_set_deterministic: null engine");
+    e->eng->set_deterministic(on != 0);
+    e->graph = false;
+  });
+}
+
 int adatm_batch_create(adatm_engine *const *engines, int n, adatm_batch **out) {
   return guarded([&] {
     if (n < 1 || !engines || !out) throw BadInput("adatm_batch_create: no engines");

@@ -166,6 +166,14 @@ void Engine::set_chunks(uint32_t chunk_leaf, uint32_t chunk_rows) {
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
+void Engine::set_deterministic(bool on) {
+  if (on == opt_.deterministic) return;
+  drop_graph();
+  opt_.deterministic = on;
+  build_walks();
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Engine::set_walkers(int walkers) {
   if (walkers != 0 && !walkers_supported((int)R_, walkers))
     throw BadInput("no contraction kernel for " + std::to_string(walkers) + " walkers at rank " +
@@ -375,6 +383,7 @@ std::unique_ptr<TreeWalk> Engine::make_walk(int mode, int g, int tag) {
   w->chunk = opt_.chunk_leaf;
   w->resident = opt_.resident_grid;
   w->walkers = opt_.walkers;
+  w->deterministic = opt_.deterministic;
   if (tag == 0 && gp.n_imten > 0) {
     // memo root: store level begin_imten-1-deg into memo tree deg
     for (uint64_t deg = 0; deg < gp.n_imten; ++deg)
@@ -471,11 +480,7 @@ void Engine::mttkrp_direct(int mode, float *out) {
               opt_.factor_type, out, stream_);
 }
 
-int Engine::kernels_per_mttkrp(int mode) const {
-  const TreeWalk &w = *walk_[mode];
-  if (w.nchunks == 0) return 0;
-  return w.has_store() ? 2 : 1;
-}
+int Engine::kernels_per_mttkrp(int mode) const { return walk_kernels(*walk_[mode]); }
 
 int Engine::kernels_per_sweep() const {
   int k = 1;  // fit

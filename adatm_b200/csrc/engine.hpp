@@ -24,6 +24,9 @@ struct EngineOptions {
   bool resident_grid = true;
   // walkers per warp in the contraction source loop (0 = default_walkers(R))
   int walkers = 0;
+  // no float atomics: every MTTKRP output and memo row is summed in an
+  // order fixed by the tree, so sweeps repeat bit for bit
+  bool deterministic = false;
 };
 
 class Engine {
@@ -116,6 +119,10 @@ class Engine {
   // Walkers per warp of the contraction walks (1, 2, 4; 0 = the default
   // for the rank); drops a captured sweep.
   void set_walkers(int walkers);
+  // Deterministic accumulation on or off (rebuilds the walks, drops a
+  // captured sweep; factors, Grams and memo rows stay).
+  void set_deterministic(bool on);
+  bool deterministic() const { return opt_.deterministic; }
   uint32_t chunk_leaf() const { return opt_.chunk_leaf; }
   uint32_t chunk_rows() const { return opt_.chunk_rows; }
   // Time `count` graph-replayed sweeps (CUDA events, ms total).

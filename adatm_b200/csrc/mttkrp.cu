@@ -29,7 +29,20 @@ struct WalkArgs {
   const uint8_t *hot_slot;     // scatter: slot of an output row summed per block, 0xFF = none
   const uint32_t *hot_rows;    // scatter: output row of each slot
   int nhot;
+  // deterministic contraction: instead of atomics, the partial sums of the
+  // nodes a chunk boundary cuts go to per-chunk rows (head: the node that
+  // began before the chunk and closes in it; tail: the node open at its
+  // end), summed later in chunk order; span_lev[l] is level l's slot
+  // (-1 = none)
+  float *span;
+  int span_nlev;
+  int span_lev[kMaxModes];
 };
+
+// Row of chunk c's head (which = 0) or tail (which = 1) partial at level l.
+__device__ __forceinline__ float *span_row(const WalkArgs &a, uint32_t c, int l, int which) {
+  return a.span + (((size_t)c * a.span_nlev + a.span_lev[l]) * 2 + which) * a.ldr;
+}
 
 constexpr int kHotRows = 32;     // output rows summed per block, at most
 constexpr uint32_t kHotMin = 32768;  // units that must hit a row to make it one
@@ -481,8 +494,9 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
         float *store = a.store[l];
         if (store != nullptr && (uint64_t)first + n <= a.nfibs[l]) {
           float *sp = store + (size_t)first * a.ldr + col;
-          if (pfirst) red_rows<V>(sp, 0, 0, 0, items[lane], act);
-          else st_rows<V>(sp, 0, 0, 0, items[lane], act);
+          if (!pfirst) st_rows<V>(sp, 0, 0, 0, items[lane], act);
+          else if (a.span) st_rows<V>(span_row(a, chunk_id, l, 0), 0, 0, col, items[lane], act);
+          else red_rows<V>(sp, 0, 0, 0, items[lane], act);
           for (int i = 1; i < n; ++i) {
             sp += a.ldr;
             st_rows<V>(sp, 0, 0, 0, items[i * 32 + lane], act);
@@ -514,9 +528,12 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
           for (int i = 0; i < n; ++i) {
             const fv<V> val = items[i * 32 + lane];
             const uint32_t orow = __shfl_sync(~0u, fid, i);
-            if (d == 0) {
-              if (i == 0 && pfirst) red_rows<V>(a.out, orow, a.ldr, col, val, act);
-              else st_rows<V>(a.out, orow, a.ldr, col, val, act);
+            if (a.out == nullptr) {
+              // deterministic d > 0: the level-d sums went to a store row
+            } else if (d == 0) {
+              if (!(i == 0 && pfirst)) st_rows<V>(a.out, orow, a.ldr, col, val, act);
+              else if (a.span) st_rows<V>(span_row(a, chunk_id, 0, 0), 0, 0, col, val, act);
+              else red_rows<V>(a.out, orow, a.ldr, col, val, act);
             } else {
               red_rows<V>(a.out, orow, a.ldr, col, fv_mul(val, pre[(d - 1) * 32 + lane]), act);
               const uint32_t ci = __shfl_sync(~0u, icd, i);
@@ -539,17 +556,24 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       const uint32_t node = __shfl_sync(~0u, nodeL, l);
       if ((uint64_t)node >= a.nfibs[l]) continue;
       const fv<V> val = carry[l * 32 + lane];
-      if (a.store[l] != nullptr) red_rows<V>(a.store[l], node, a.ldr, col, val, act);
+      if (a.store[l] != nullptr) {
+        if (a.span) st_rows<V>(span_row(a, chunk_id, l, 1), 0, 0, col, val, act);
+        else red_rows<V>(a.store[l], node, a.ldr, col, val, act);
+      }
       if (l > d) {
         const fv<V> r = ld_factor<V, FT>(a.U[l], __ldg(a.fids[l] + node), a.ldr, col, act);
         fv<V> c2 = carry[(l - 1) * 32 + lane];
         fv_fma(c2, val, r);
         carry[(l - 1) * 32 + lane] = c2;
         touched |= 1u << (l - 1);
-      } else {
-        const uint32_t orow = __ldg(a.fids[d] + node);
-        red_rows<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
-                    act);
+      } else if (a.out != nullptr) {
+        if (a.span && d == 0) {
+          st_rows<V>(span_row(a, chunk_id, 0, 1), 0, 0, col, val, act);
+        } else {
+          const uint32_t orow = __ldg(a.fids[d] + node);
+          red_rows<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
+                      act);
+        }
       }
     }
     __syncwarp();
@@ -813,6 +837,186 @@ __global__ void k_prezero(WalkArgs a, const uint32_t *sched) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Deterministic accumulation: chain sums of cut nodes, prefix rows, pulls.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kChainGroup = 32;  // partials one warp sums per group
+constexpr uint32_t kPullSeg = 256;    // units per pull segment (whole rows) and per piece
+
+struct ChainArgs {
+  const float *span;
+  int span_nlev, ldr, R;
+  int span_lev[kMaxModes];
+  const uint32_t *chains;  // 6 per chain
+  const uint32_t *groups;  // 3 per group
+  uint32_t nchains, ngroups;
+  float *gsum;
+  float *store[kMaxModes];
+  float *out;              // level-0 output rows (output level 0), else nullptr
+  const uint32_t *root_ids;
+};
+
+// Partial k of the chain of a node cut by the boundaries of chunks
+// c_first..c_last: k <= c_last - c_first is the tail of chunk c_first-1+k,
+// the last one the head of chunk c_last (where the node closes).
+__device__ __forceinline__ const float *chain_partial(const ChainArgs &a, int ls, uint32_t c_first,
+                                                      uint32_t c_last, uint32_t k) {
+  const uint32_t ntail = c_last - c_first + 1;
+  const uint32_t c = k < ntail ? c_first - 1 + k : c_last;
+  const int which = k < ntail ? 1 : 0;
+  return a.span + (((size_t)c * a.span_nlev + ls) * 2 + which) * a.ldr;
+}
+
+// One warp per group: its partials summed in chunk order.
+__global__ void k_chain_groups(const __grid_constant__ ChainArgs a) {
+  const uint32_t g = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (g >= a.ngroups) return;
+  const uint32_t ch = a.groups[3 * (size_t)g], k0 = a.groups[3 * (size_t)g + 1],
+                 cnt = a.groups[3 * (size_t)g + 2];
+  const uint32_t *c = a.chains + 6 * (size_t)ch;
+  const int ls = a.span_lev[c[0]];
+  for (int col = lane; col < a.R; col += 32) {
+    float acc = 0.f;
+    for (uint32_t k = k0; k < k0 + cnt; ++k) acc += chain_partial(a, ls, c[2], c[3], k)[col];
+    a.gsum[(size_t)g * a.ldr + col] = acc;
+  }
+}
+
+// One warp per chain: the group sums in order, stored to the node's memo row
+// and, at level 0 with a root output, to its output row.
+__global__ void k_chain_finish(const __grid_constant__ ChainArgs a) {
+  const uint32_t ch = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (ch >= a.nchains) return;
+  const uint32_t *c = a.chains + 6 * (size_t)ch;
+  const int l = (int)c[0];
+  const uint32_t node = c[1], g0 = c[4], ng = c[5];
+  float *st = a.store[l];
+  float *ot = (l == 0 && a.out) ? a.out + (size_t)a.root_ids[node] * a.ldr : nullptr;
+  for (int col = lane; col < a.R; col += 32) {
+    float acc = 0.f;
+    for (uint32_t g = g0; g < g0 + ng; ++g) acc += a.gsum[(size_t)g * a.ldr + col];
+    if (st) st[(size_t)node * a.ldr + col] = acc;
+    if (ot) ot[col] = acc;
+  }
+}
+
+// parent[c] = p for the children c of every node p (fptr of the parent level).
+__global__ void k_fill_parent(const uint32_t *fptr, uint64_t nparent, uint32_t *parent) {
+  for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < nparent;
+       p += (uint64_t)gridDim.x * blockDim.x)
+    for (uint32_t c = fptr[p]; c < fptr[p + 1]; ++c) parent[c] = (uint32_t)p;
+}
+
+// Prefix rows of one level: P_l[n] = P_{l-1}[parent(n)] * U_l[fids_l[n]]
+// (P_0[n] = U_0[fids_0[n]]); padding columns are zero.
+template <FactorType FT>
+__global__ void k_prefix_level(const void *U, const uint32_t *fids, const uint32_t *parent,
+                               const float *prev, uint64_t n, int R, int ldr, float *out) {
+  const int q = ldr / 4;
+  const uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (e >= n * (uint64_t)q) return;
+  const uint64_t node = e / q;
+  const int col = 4 * (int)(e % q);
+  const fv<4> u = ld_factor<4, FT>(U, fids[node], ldr, col, col < R);
+  float4 r = make_float4(u.x[0], u.x[1], u.x[2], u.x[3]);
+  if (prev) {
+    const float4 p = *reinterpret_cast<const float4 *>(prev + (size_t)parent[node] * ldr + col);
+    r = make_float4(r.x * p.x, r.y * p.y, r.z * p.z, r.w * p.w);
+  }
+  *reinterpret_cast<float4 *>(out + node * ldr + col) = r;
+}
+
+struct PullArgs {
+  int d, R, ldr;
+  const uint32_t *perm, *prow, *pparent, *segs;
+  uint32_t nsegs;
+  const float *vals;      // leaf values (leaf source)
+  const float *src_rows;  // node rows of level d (row source)
+  const float *prefix;    // P_{d-1} rows (d >= 1)
+  float *out;
+  float *piece_sum;
+};
+
+// Pull scatter: one warp per segment of units sorted by output row; each
+// unit's contribution src(u) * P_{d-1}[parent(u)] is added in that order and
+// a row is stored once, when its last unit is done (whole rows), or into its
+// piece's slot (long rows, summed in order by k_piece_sum).
+template <int V, bool LEAF>
+__global__ void __launch_bounds__(256) k_pull(const __grid_constant__ PullArgs a) {
+  __shared__ uint4 stage[kWarps][kBatch];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int col = lane * V;
+  const bool act = col < a.R;
+  constexpr int SB = 8;
+  for (uint32_t sg = blockIdx.x * kWarps + warp; sg < a.nsegs; sg += gridDim.x * kWarps) {
+    const uint32_t jb = a.segs[3 * (size_t)sg], je = a.segs[3 * (size_t)sg + 1],
+                   slot = a.segs[3 * (size_t)sg + 2];
+    fv<V> acc = fv_fill<V>(0.f);
+    uint32_t cur = a.prow[jb];
+    auto flush = [&](uint32_t row) {
+      if (slot == 0xFFFFFFFFu) st_rows<V>(a.out, row, a.ldr, col, acc, act);
+      else st_rows<V>(a.piece_sum, slot, a.ldr, col, acc, act);
+    };
+    for (uint32_t j0 = jb; j0 < je; j0 += kBatch) {
+      const int cnt = (int)min((uint32_t)kBatch, je - j0);
+      if (lane < cnt) {
+        const uint32_t u = a.perm[j0 + lane];
+        const float v = LEAF ? a.vals[u] : 0.f;
+        stage[warp][lane] = make_uint4(u, a.prow[j0 + lane], a.d >= 1 ? a.pparent[j0 + lane] : 0u,
+                                       __float_as_uint(v));
+      }
+      __syncwarp();
+      for (int k0 = 0; k0 < cnt; k0 += SB) {
+        fv<V> x[SB];
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const int k = k0 + q;
+          const bool ok = k < cnt;
+          const uint4 e = stage[warp][ok ? k : 0];
+          fv<V> t;
+          if constexpr (LEAF) t = fv_fill<V>(__uint_as_float(e.w));
+          else t = ld_rows<V>(a.src_rows, e.x, a.ldr, col, ok && act);
+          if (a.d >= 1) t = fv_mul(t, ld_rows<V>(a.prefix, e.z, a.ldr, col, ok && act));
+          x[q] = t;
+        }
+#pragma unroll
+        for (int q = 0; q < SB; ++q) {
+          const int k = k0 + q;
+          if (k < cnt) {
+            const uint32_t row = stage[warp][k].y;
+            if (row != cur) {
+              flush(cur);
+              acc = fv_fill<V>(0.f);
+              cur = row;
+            }
+#pragma unroll
+            for (int i = 0; i < V; ++i) acc.x[i] += x[q].x[i];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    flush(cur);
+  }
+}
+
+// One warp per long row: its pieces summed in order.
+__global__ void k_piece_sum(const uint32_t *pieces, uint32_t nlong, const float *piece_sum, int R,
+                            int ldr, float *out) {
+  const uint32_t i = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= nlong) return;
+  const uint32_t row = pieces[3 * (size_t)i], p0 = pieces[3 * (size_t)i + 1],
+                 np = pieces[3 * (size_t)i + 2];
+  for (int col = lane; col < R; col += 32) {
+    float acc = 0.f;
+    for (uint32_t p = p0; p < p0 + np; ++p) acc += piece_sum[(size_t)p * ldr + col];
+    out[(size_t)row * ldr + col] = acc;
+  }
+}
+
 WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   WalkArgs a;
   const DevCsf &c = *w.csf;
@@ -842,6 +1046,9 @@ WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   a.nhot = w.nhot;
   a.hot_slot = w.hot_slot.get();
   a.hot_rows = w.hot_rows.get();
+  a.span = w.deterministic ? w.span.get() : nullptr;
+  a.span_nlev = w.span_nlev;
+  for (int l = 0; l < kMaxModes; ++l) a.span_lev[l] = w.span_lev[l];
   return a;
 }
 
@@ -1007,6 +1214,248 @@ void set_walk_attributes() {
   done = true;
 }
 
+// ---------------------------------------------------------------------------
+// Deterministic walks: preparation and launch.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <typename T>
+std::vector<T> to_host(const T *dev, size_t n, cudaStream_t s) {
+  std::vector<T> h(n);
+  if (n) ADATM_CUDA(cudaMemcpyAsync(h.data(), dev, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  ADATM_CUDA(cudaStreamSynchronize(s));
+  return h;
+}
+
+template <typename T>
+void to_device(DevBuf<T> &dst, const std::vector<T> &h, cudaStream_t s) {
+  dst.alloc(std::max<size_t>(h.size(), 1));
+  if (!h.empty())
+    ADATM_CUDA(cudaMemcpyAsync(dst.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  ADATM_CUDA(cudaStreamSynchronize(s));
+}
+
+// Slots and chains of a contraction: levels whose cut nodes would take
+// atomics (stored levels, and level 0 when it is the output), and for each
+// node a chunk boundary cuts, the run of chunks it spans.
+void det_prepare_contract(TreeWalk &w, cudaStream_t s) {
+  const DevCsf &c = *w.csf;
+  const int S = w.src, d = w.out;
+  if (d > 0) {
+    // the level-d sums are stored, then pulled into the output rows
+    w.level_rows.alloc((size_t)std::max<uint64_t>(c.nfibs[d], 1) * w.ldr);
+    ADATM_CUDA(cudaMemsetAsync(w.level_rows.get(), 0, w.level_rows.bytes(), s));
+    w.store[d] = w.level_rows.get();
+    w.pull = true;
+  }
+  w.span_nlev = 0;
+  for (int l = 0; l < kMaxModes; ++l) w.span_lev[l] = -1;
+  for (int l = 0; l < S; ++l)
+    if (w.store[l] != nullptr || (l == 0 && d == 0)) w.span_lev[l] = w.span_nlev++;
+  w.nchains = w.ngroups = 0;
+  if (w.nchunks == 0 || w.span_nlev == 0) return;
+  w.span.alloc((size_t)w.nchunks * w.span_nlev * 2 * w.ldr);
+  const std::vector<uint32_t> sc = to_host(w.sched.get(), (size_t)w.nchunks * (S + 1), s);
+  std::vector<uint32_t> chains, groups;
+  const size_t st = (size_t)S + 1;
+  for (int l = 0; l < S; ++l) {
+    if (w.span_lev[l] < 0) continue;
+    uint32_t ch = 1;
+    while (ch < w.nchunks) {
+      if (!((sc[ch * st + S] >> l) & 1u)) {
+        ++ch;
+        continue;
+      }
+      const uint32_t node = sc[ch * st + l];
+      uint32_t last = ch;
+      while (last + 1 < w.nchunks && ((sc[(last + 1) * st + S] >> l) & 1u) &&
+             sc[(last + 1) * st + l] == node)
+        ++last;
+      const uint32_t npart = (last - ch + 1) + 1;
+      const uint32_t id = (uint32_t)(chains.size() / 6);
+      const uint32_t g0 = (uint32_t)(groups.size() / 3);
+      const uint32_t ng = (npart + kChainGroup - 1) / kChainGroup;
+      for (uint32_t k0 = 0; k0 < npart; k0 += kChainGroup) {
+        groups.push_back(id);
+        groups.push_back(k0);
+        groups.push_back(std::min(kChainGroup, npart - k0));
+      }
+      const uint32_t row[6] = {(uint32_t)l, node, ch, last, g0, ng};
+      chains.insert(chains.end(), row, row + 6);
+      ch = last + 1;
+    }
+  }
+  w.nchains = (uint32_t)(chains.size() / 6);
+  w.ngroups = (uint32_t)(groups.size() / 3);
+  to_device(w.chains, chains, s);
+  to_device(w.groups, groups, s);
+  w.gsum.alloc((size_t)std::max<uint32_t>(w.ngroups, 1) * w.ldr);
+}
+
+// The pull of level d = w.out: units (level-d nodes) in a stable order by
+// output row, their parents, segments of whole rows and pieces of long rows,
+// the parent arrays and prefix buffers of the levels above.
+void det_prepare_pull(TreeWalk &w, cudaStream_t s) {
+  const DevCsf &c = *w.csf;
+  const int d = w.out;
+  const uint64_t n = c.nfibs[d];
+  const uint64_t rows = c.dims[c.dim_perm[d]];
+  const std::vector<uint32_t> fid = to_host(c.fids[d].get(), n, s);
+  std::vector<uint32_t> par;
+  if (d >= 1) {
+    const std::vector<uint32_t> fp = to_host(c.fptr[d - 1].get(), c.nfibs[d - 1] + 1, s);
+    par.assign(n, 0);
+    for (uint64_t p = 0; p < c.nfibs[d - 1]; ++p)
+      for (uint32_t u = fp[p]; u < fp[p + 1] && u < n; ++u) par[u] = (uint32_t)p;
+  }
+  // stable counting sort by output row
+  std::vector<uint64_t> start(rows + 1, 0);
+  for (uint64_t u = 0; u < n; ++u) ++start[fid[u] + 1];
+  for (uint64_t r = 0; r < rows; ++r) start[r + 1] += start[r];
+  std::vector<uint32_t> perm(n), prow(n), pparent(d >= 1 ? n : 0);
+  {
+    std::vector<uint64_t> pos(start.begin(), start.end() - 1);
+    for (uint64_t u = 0; u < n; ++u) {
+      const uint64_t j = pos[fid[u]]++;
+      perm[j] = (uint32_t)u;
+      prow[j] = fid[u];
+      if (d >= 1) pparent[j] = par[u];
+    }
+  }
+  // segments: whole rows packed up to kPullSeg units; longer rows in pieces
+  std::vector<uint32_t> segs, pieces;
+  uint32_t npieces = 0;
+  uint64_t seg_start = 0, seg_len = 0;
+  auto close_seg = [&](uint64_t end) {
+    if (seg_len > 0) {
+      segs.push_back((uint32_t)seg_start);
+      segs.push_back((uint32_t)end);
+      segs.push_back(0xFFFFFFFFu);
+    }
+    seg_start = end;
+    seg_len = 0;
+  };
+  for (uint64_t r = 0; r < rows; ++r) {
+    const uint64_t b = start[r], cnt = start[r + 1] - b;
+    if (cnt == 0) continue;
+    if (cnt > kPullSeg) {
+      close_seg(b);
+      const uint32_t np = (uint32_t)((cnt + kPullSeg - 1) / kPullSeg);
+      pieces.push_back((uint32_t)r);
+      pieces.push_back(npieces);
+      pieces.push_back(np);
+      for (uint32_t q = 0; q < np; ++q) {
+        segs.push_back((uint32_t)(b + (uint64_t)q * kPullSeg));
+        segs.push_back((uint32_t)std::min<uint64_t>(b + (uint64_t)(q + 1) * kPullSeg, b + cnt));
+        segs.push_back(npieces + q);
+      }
+      npieces += np;
+      seg_start = b + cnt;
+      continue;
+    }
+    if (seg_len + cnt > kPullSeg) close_seg(b);
+    seg_len += cnt;
+  }
+  close_seg(n);
+  w.nsegs = (uint32_t)(segs.size() / 3);
+  w.nlong = (uint32_t)(pieces.size() / 3);
+  w.npieces = npieces;
+  to_device(w.perm, perm, s);
+  to_device(w.prow, prow, s);
+  to_device(w.pparent, pparent, s);
+  to_device(w.segs, segs, s);
+  to_device(w.pieces, pieces, s);
+  w.piece_sum.alloc((size_t)std::max<uint32_t>(npieces, 1) * w.ldr);
+  // parents and prefix rows of levels 1..d-1
+  uint64_t maxf = 1;
+  for (int l = 0; l < d; ++l) maxf = std::max<uint64_t>(maxf, c.nfibs[l]);
+  for (int l = 1; l < d; ++l) {
+    w.parent[l].alloc(std::max<uint64_t>(c.nfibs[l], 1));
+    const uint64_t np = c.nfibs[l - 1];
+    if (np == 0) continue;
+    k_fill_parent<<<(unsigned)std::min<uint64_t>((np + 255) / 256, 65535), 256, 0, s>>>(
+        c.fptr[l - 1].get(), np, w.parent[l].get());
+    ADATM_LAUNCH();
+  }
+  if (d >= 1) w.prefix[0].alloc(maxf * w.ldr);
+  if (d >= 2) w.prefix[1].alloc(maxf * w.ldr);
+  ADATM_CUDA(cudaStreamSynchronize(s));
+}
+
+template <FactorType FT>
+void launch_prefix(const TreeWalk &w, const LevelFactors &f, cudaStream_t s) {
+  const DevCsf &c = *w.csf;
+  for (int l = 0; l < w.out; ++l) {
+    const uint64_t n = c.nfibs[l];
+    if (n == 0) continue;
+    const uint64_t thr = n * (uint64_t)(w.ldr / 4);
+    k_prefix_level<FT><<<(unsigned)((thr + 255) / 256), 256, 0, s>>>(
+        f.U[l], c.fids[l].get(), l ? w.parent[l].get() : nullptr,
+        l ? w.prefix[(l - 1) & 1].get() : nullptr, n, w.R, w.ldr, w.prefix[l & 1].get());
+    ADATM_LAUNCH();
+  }
+}
+
+void launch_pull(const TreeWalk &w, const LevelFactors &f, FactorType ft, const float *rows,
+                 float *out, cudaStream_t s) {
+  if (w.nsegs == 0) return;
+  if (ft == FactorType::F32) launch_prefix<FactorType::F32>(w, f, s);
+  else launch_prefix<FactorType::BF16>(w, f, s);
+  PullArgs a;
+  a.d = w.out;
+  a.R = w.R;
+  a.ldr = w.ldr;
+  a.perm = w.perm.get();
+  a.prow = w.prow.get();
+  a.pparent = w.pparent.get();
+  a.segs = w.segs.get();
+  a.nsegs = w.nsegs;
+  a.vals = w.csf->vals32.get();
+  a.src_rows = rows;
+  a.prefix = w.out >= 1 ? w.prefix[(w.out - 1) & 1].get() : nullptr;
+  a.out = out;
+  a.piece_sum = w.piece_sum.get();
+  const bool leaf = rows == nullptr;
+  const unsigned blocks = (w.nsegs + kWarps - 1) / kWarps;
+  switch (vec_for_rank(w.R)) {
+    case 1: leaf ? k_pull<1, true><<<blocks, 256, 0, s>>>(a) : k_pull<1, false><<<blocks, 256, 0, s>>>(a); break;
+    case 2: leaf ? k_pull<2, true><<<blocks, 256, 0, s>>>(a) : k_pull<2, false><<<blocks, 256, 0, s>>>(a); break;
+    default: leaf ? k_pull<4, true><<<blocks, 256, 0, s>>>(a) : k_pull<4, false><<<blocks, 256, 0, s>>>(a); break;
+  }
+  ADATM_LAUNCH();
+  if (w.nlong) {
+    k_piece_sum<<<(w.nlong * 32 + 255) / 256, 256, 0, s>>>(w.pieces.get(), w.nlong, w.piece_sum.get(),
+                                                             w.R, w.ldr, out);
+    ADATM_LAUNCH();
+  }
+}
+
+void launch_chains(const TreeWalk &w, float *out, cudaStream_t s) {
+  if (w.nchains == 0) return;
+  ChainArgs a;
+  a.span = w.span.get();
+  a.span_nlev = w.span_nlev;
+  a.ldr = w.ldr;
+  a.R = w.R;
+  for (int l = 0; l < kMaxModes; ++l) {
+    a.span_lev[l] = w.span_lev[l];
+    a.store[l] = w.store[l];
+  }
+  a.chains = w.chains.get();
+  a.groups = w.groups.get();
+  a.nchains = w.nchains;
+  a.ngroups = w.ngroups;
+  a.gsum = w.gsum.get();
+  a.out = w.out == 0 ? out : nullptr;
+  a.root_ids = w.csf->fids[0].get();
+  k_chain_groups<<<(unsigned)(((uint64_t)w.ngroups * 32 + 255) / 256), 256, 0, s>>>(a);
+  ADATM_LAUNCH();
+  k_chain_finish<<<(unsigned)(((uint64_t)w.nchains * 32 + 255) / 256), 256, 0, s>>>(a);
+  ADATM_LAUNCH();
+}
+
+}  // namespace
+
 // The output rows of a scatter walk hit by the most units (at most
 // kHotRows, each by at least kHotMin units), and the row -> slot table.
 void find_hot_rows(TreeWalk &w, cudaStream_t s) {
@@ -1059,14 +1508,24 @@ void walk_prepare(TreeWalk &w, cudaStream_t s) {
   WalkArgs a = make_args(w, nullptr, nullptr);
   k_schedule<<<(w.nchunks + 255) / 256, 256, 0, s>>>(a, w.sched.get());
   ADATM_LAUNCH();
+  if (w.deterministic) {
+    w.pull = w.src == w.out;
+    if (w.src > w.out) det_prepare_contract(w, s);
+    if (w.pull) det_prepare_pull(w, s);
+    return;
+  }
   if (w.src == w.out && w.nunits >= kHotMin) find_hot_rows(w, s);
 }
 
 void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float *out,
                  cudaStream_t s) {
   if (w.nchunks == 0) return;
-  const WalkArgs a = make_args(w, &f, out);
-  if (w.has_store()) {
+  if (w.deterministic && w.src == w.out) {
+    launch_pull(w, f, ft, w.src == w.nmodes - 1 ? nullptr : w.src_rows, out, s);
+    return;
+  }
+  const WalkArgs a = make_args(w, &f, w.deterministic && w.out > 0 ? nullptr : out);
+  if (w.has_store() && !w.deterministic) {
     dim3 blk(32, 8);
     k_prezero<<<(w.nchunks + 7) / 8, blk, 0, s>>>(a, w.sched.get());
     ADATM_LAUNCH();
@@ -1083,6 +1542,10 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
       if (leaf) launch_contract<FactorType::BF16, true>(vec, wk, a, blocks, w.resident, s);
       else launch_contract<FactorType::BF16, false>(vec, wk, a, blocks, w.resident, s);
     }
+    if (w.deterministic) {
+      launch_chains(w, out, s);
+      if (w.pull) launch_pull(w, f, ft, w.level_rows.get(), out, s);
+    }
   } else {
     const int lanes = lanes_for_rank(w.R);
     if (ft == FactorType::F32) {
@@ -1093,6 +1556,19 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
       else launch_scatter<FactorType::BF16, false>(lanes, a, blocks, s);
     }
   }
+}
+
+int walk_kernels(const TreeWalk &w) {
+  if (w.nchunks == 0) return 0;
+  int k = 0;
+  if (w.src > w.out) {
+    k += 1;                                            // the contraction
+    if (!w.deterministic) return k + (w.has_store() ? 1 : 0);  // + the prezero of cut memo rows
+    if (w.nchains) k += 2;                             // chain groups, chain finish
+  }
+  if (w.deterministic && w.pull && w.nsegs) k += w.out + 1 + (w.nlong ? 1 : 0);
+  if (!w.deterministic && w.src == w.out) k += 1;      // the scatter
+  return k;
 }
 
 double walk_compulsory_bytes(const TreeWalk &w, FactorType ft, const uint64_t *dims_of_level,

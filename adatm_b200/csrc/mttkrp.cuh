@@ -57,12 +57,42 @@ struct TreeWalk {
   int nhot = 0;
   DevBuf<uint8_t> hot_slot;
   DevBuf<uint32_t> hot_rows;
+  // Deterministic accumulation (no float atomics): every output and memo
+  // row is summed in an order fixed by the tree, so repeated runs agree bit
+  // for bit. Contractions write the partial sums of the nodes chunk
+  // boundaries cut to per-chunk rows (span) and sum them per node in chunk
+  // order (chains, in groups of kChainGroup partials); scatters, and the
+  // output of contractions below the root, pull each output row's units in
+  // the order of a stable sort by output row (segments of whole rows, long
+  // rows split into pieces summed in order).
+  bool deterministic = false;
+  int span_nlev = 0;
+  int span_lev[kMaxModes] = {-1, -1, -1, -1, -1, -1, -1, -1};
+  DevBuf<float> span;                // nchunks x span_nlev x 2 x ldr
+  DevBuf<uint32_t> chains;           // per chain: level, node, first boundary chunk, last chunk,
+                                     // first group, groups
+  DevBuf<uint32_t> groups;           // per group: chain, first partial, partials
+  DevBuf<float> gsum;                // per group: its sum (ldr)
+  uint32_t nchains = 0, ngroups = 0;
+  DevBuf<float> level_rows;          // contraction below the root: level-d node sums
+  // pull scatter of level `out` (deterministic scatters and contractions below the root)
+  bool pull = false;
+  DevBuf<uint32_t> parent[kMaxModes];  // parent node of every node of levels 1..out
+  DevBuf<uint32_t> perm, prow, pparent;  // units sorted by output row (stable), their rows, parents
+  DevBuf<uint32_t> segs;             // per segment: first, end, piece slot (~0u: whole rows)
+  DevBuf<uint32_t> pieces;           // per long row: row, first piece slot, pieces
+  DevBuf<float> piece_sum;           // per piece: its sum (ldr)
+  uint32_t nsegs = 0, nlong = 0, npieces = 0;
+  DevBuf<float> prefix[2];           // prefix rows of levels 0..out-1 (ping-pong)
   bool has_store() const {
     for (int l = 0; l < kMaxModes; ++l)
       if (store[l]) return true;
     return false;
   }
 };
+
+// Kernel launches of one walk (for launch counts).
+int walk_kernels(const TreeWalk &w);
 
 // Walkers per warp of the contraction's source loop by default at rank R,
 // and whether W walkers are built for rank R.
@@ -74,7 +104,7 @@ bool walkers_supported(int R, int W);
 void walk_prepare(TreeWalk &w, cudaStream_t s);
 
 // Launch the walk: output rows must be zero beforehand (the caller clears
-// them); memo rows cut by chunk boundaries are zeroed here.
+// them); memo rows cut by chunk boundaries are zeroed here (atomic mode).
 void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float *out,
                  cudaStream_t s);
 
