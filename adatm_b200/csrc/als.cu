@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int
 // per-block FP64 partial Gram and column maxima of A_raw.
 // ---------------------------------------------------------------------------
 struct UpdArgs {
+  int split;           // Gram products as 3 TF32 terms (FP32 rows) or 1 (BF16-valued rows)
   const float *M;
   const double *vinv;  // R x R fp64, or nullptr for identity
   float *A;           // output rows (may alias M when vinv == nullptr)
@@ -148,15 +149,45 @@ struct UpdArgs {
   double *part_max;   // gridDim x R
 };
 
+// One m16n8k8 TF32 tensor-core product with FP32 accumulation, c += a * b
+// (A 16 x 8 row-major, B 8 x 8 column-major, per-thread fragments of the
+// warp-wide tiles).
+__device__ __forceinline__ void mma_tf32(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+      "{%8,%9}, {%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// Row pass of a mode update (or of a plain Gram). Each block takes row
+// groups of 256 / LANES rows; the rows (A = M V^-1, or M itself) are staged
+// in shared memory and their Gram X^T X is taken on the tensor cores: G is
+// tiled in 16 x 8 tiles spread over the block's 8 warps, each tile a chain of
+// m16n8k8 TF32 MMAs over the group's rows with FP32 accumulation, added to
+// FP64 per-thread sums after every group. FP32 rows split into a TF32 big
+// part and a TF32 remainder, and big*big + big*rem + rem*big keeps the
+// products to ~2^-22 (split = 1); BF16-valued rows are exact in TF32 and
+// take one product.
 template <int LANES>
 __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
   constexpr int GROUPS = 256 / LANES;
   constexpr int RMAX = 4 * LANES;
-  constexpr int PAIRS = (RMAX * RMAX + 255) / 256;
+  constexpr int RS = RMAX + 8;          // staged row stride (bank-conflict free MMA loads)
+  constexpr int TN = RMAX / 8;          // 8-column tiles of G
+  constexpr int NT = (RMAX / 16) * TN;  // 16 x 8 tiles
+  constexpr int TPW = (NT + 7) / 8;     // tiles per warp
   extern __shared__ double usm[];
   double *vinv = usm;                                            // RMAX x RMAX
-  float *rowbuf = reinterpret_cast<float *>(usm + RMAX * RMAX);  // GROUPS x RMAX
+  float *rowbuf = reinterpret_cast<float *>(usm + RMAX * RMAX);  // GROUPS x RS
   const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
   const int g = tid / LANES, t = tid % LANES, col = 4 * t;
   const int R = a.R;
   const bool act = col < R;
@@ -168,9 +199,11 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
       vinv[e] = (k < R && c < R) ? a.vinv[k * R + c] : 0.0;
     }
   }
-  double gacc[PAIRS];
+  double gacc[TPW][4];
 #pragma unroll
-  for (int p = 0; p < PAIRS; ++p) gacc[p] = 0.0;
+  for (int tt = 0; tt < TPW; ++tt)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) gacc[tt][q] = 0.0;
   double cmax = 0.0;
   __syncthreads();
   const int kq = (R + 3) / 4;
@@ -207,28 +240,55 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
     } else {
       o = m;
     }
-    *reinterpret_cast<float4 *>(rowbuf + g * RMAX + col) =
+    *reinterpret_cast<float4 *>(rowbuf + g * RS + col) =
         valid ? o : make_float4(0.f, 0.f, 0.f, 0.f);
     __syncthreads();
 #pragma unroll
-    for (int p = 0; p < PAIRS; ++p) {
-      const int pair = tid + p * 256;
-      if (pair < R * R) {
-        const int r = pair / R, s2 = pair % R;
-        double acc = 0.0;
-        for (int gi = 0; gi < GROUPS; ++gi)
-          acc += (double)rowbuf[gi * RMAX + r] * (double)rowbuf[gi * RMAX + s2];
-        gacc[p] += acc;
+    for (int tt = 0; tt < TPW; ++tt) {
+      const int tile = warp + 8 * tt;
+      const int i0 = (tile / TN) * 16, j0 = (tile % TN) * 8;
+      if (tile < NT && i0 < R && j0 < R) {
+        float c[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k0 = 0; k0 < GROUPS; k0 += 8) {
+          // A = X^T (rows i0.., the group's rows as k), B = X (columns j0..)
+          const float *x0 = rowbuf + (k0 + tig) * RS, *x1 = rowbuf + (k0 + tig + 4) * RS;
+          const float av[4] = {x0[i0 + gid], x0[i0 + gid + 8], x1[i0 + gid], x1[i0 + gid + 8]};
+          const float bv[2] = {x0[j0 + gid], x1[j0 + gid]};
+          uint32_t ab[4], bb[2];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) ab[q] = to_tf32(av[q]);
+          bb[0] = to_tf32(bv[0]);
+          bb[1] = to_tf32(bv[1]);
+          mma_tf32(c, ab, bb);
+          if (a.split) {
+            uint32_t as[4], bs[2];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) as[q] = to_tf32(av[q] - __uint_as_float(ab[q]));
+            bs[0] = to_tf32(bv[0] - __uint_as_float(bb[0]));
+            bs[1] = to_tf32(bv[1] - __uint_as_float(bb[1]));
+            mma_tf32(c, ab, bs);
+            mma_tf32(c, as, bb);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gacc[tt][q] += (double)c[q];
       }
     }
     if (tid < R)
-      for (int gi = 0; gi < GROUPS; ++gi) cmax = fmax(cmax, (double)rowbuf[gi * RMAX + tid]);
+      for (int gi = 0; gi < GROUPS; ++gi) cmax = fmax(cmax, (double)rowbuf[gi * RS + tid]);
     __syncthreads();
   }
 #pragma unroll
-  for (int p = 0; p < PAIRS; ++p) {
-    const int pair = tid + p * 256;
-    if (pair < R * R) a.part_gram[(size_t)blockIdx.x * R * R + pair] = gacc[p];
+  for (int tt = 0; tt < TPW; ++tt) {
+    const int tile = warp + 8 * tt;
+    const int i0 = (tile / TN) * 16, j0 = (tile % TN) * 8;
+    if (tile >= NT || i0 >= R || j0 >= R) continue;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = i0 + gid + (q >= 2 ? 8 : 0), j = j0 + 2 * tig + (q & 1);
+      if (i < R && j < R) a.part_gram[(size_t)blockIdx.x * R * R + i * R + j] = gacc[tt][q];
+    }
   }
   if (tid < R) a.part_max[(size_t)blockIdx.x * R + tid] = cmax;
 }
@@ -407,7 +467,7 @@ int lanes_for(int R) {
 template <int LANES>
 constexpr size_t update_smem() {
   return (size_t)(4 * LANES * 4 * LANES) * sizeof(double) +
-         (size_t)((256 / LANES) * 4 * LANES) * sizeof(float);
+         (size_t)((256 / LANES) * (4 * LANES + 8)) * sizeof(float);
 }
 
 template <int LANES>
@@ -472,8 +532,10 @@ void to_bf16(float *A, __nv_bfloat16 *Ab, uint64_t rows, int ldr, cudaStream_t s
   ADATM_LAUNCH();
 }
 
-void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, cudaStream_t s) {
+void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, cudaStream_t s,
+          bool bf16_rows) {
   UpdArgs u;
+  u.split = bf16_rows ? 0 : 1;
   u.M = A;
   u.vinv = nullptr;
   u.A = nullptr;
@@ -508,6 +570,7 @@ void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s) {
 void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
                    bool inner, AlsWork &w, cudaStream_t s) {
   UpdArgs u;
+  u.split = 1;
   u.M = M;
   u.vinv = w.vinv64.get();
   u.A = A;
@@ -532,7 +595,7 @@ void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, d
   // BF16 factors were rounded after the Gram was taken: take it again from
   // the rounded rows, so the next modes' normal equations use the factor the
   // MTTKRPs read
-  if (Ab) gram(A, rows, w.R, w.ldr, G_mode, w, s);
+  if (Ab) gram(A, rows, w.R, w.ldr, G_mode, w, s, true);
 }
 
 void fit(const GramSet &g, AlsWork &w, cudaStream_t s) {
@@ -612,6 +675,7 @@ void gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, cuda
   if (((uintptr_t)A & 15) != 0) throw BadInput("adatm_gram_noalloc: A must be 16-byte aligned");
   double *scratch = noalloc_scratch();
   UpdArgs u;
+  u.split = 1;
   u.M = A;
   u.vinv = nullptr;
   u.A = nullptr;

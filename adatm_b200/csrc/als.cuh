@@ -32,8 +32,11 @@ struct GramSet {
 // uniform [0,1) from mix64(mix64(seed * 0x100000001B3 + m) + i * R + r).
 void factor_init_device(float *A, __nv_bfloat16 *Ab, uint64_t rows, int R, int ldr, uint64_t seed,
                         uint64_t mode, cudaStream_t s);
-// G = A^T A in FP64 (R x R).
-void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, cudaStream_t s);
+// G = A^T A (R x R, FP64 result): TF32 tensor-core tiles with FP32
+// accumulation per row group, FP64 across groups; FP32 rows take three TF32
+// products (big/remainder split), BF16-valued rows (bf16_rows) one exact one.
+void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, cudaStream_t s,
+          bool bf16_rows = false);
 // sum of squares of the tensor values -> w.scalars[0]
 void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s);
 // V = Hadamard of all G[n], n != mode; write V^-1 (fp64).

@@ -603,7 +603,8 @@ void Engine::get_lambda(double *host) const {
 
 void Engine::als_begin() {
   for (int m = 0; m < coo_->nmodes; ++m)
-    gram(A_[m].get(), coo_->dims[m], (int)R_, ldr_, G_[m].get(), w_, stream_);
+    gram(A_[m].get(), coo_->dims[m], (int)R_, ldr_, G_[m].get(), w_, stream_,
+         opt_.factor_type == FactorType::BF16);
   if (!ttnorm_ready_) {
     frob_sq(csf_[0]->vals64.get(), coo_->nnz, w_, stream_);
     ttnorm_ready_ = true;
