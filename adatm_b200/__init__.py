@@ -762,6 +762,30 @@ class Engine:
         _check(lib().adatm_engine_set_resident_grid(self._h, int(bool(on))),
                "adatm_engine_set_resident_grid")
 
+    # one shard of a tensor split across ranks (adatm_b200.shard)
+    def mttkrp_into(self, mode, dev_ptr):
+        """This shard's MTTKRP of `mode` into a device buffer (dims[mode] x ldr FP32)."""
+        _check(lib().adatm_engine_mttkrp_into(self._h, mode, C.c_void_p(dev_ptr)),
+               "adatm_engine_mttkrp_into")
+
+    def update_from(self, mode, dev_ptr):
+        """The mode's update from the summed MTTKRP in a device buffer."""
+        _check(lib().adatm_engine_update_from(self._h, mode, C.c_void_p(dev_ptr)),
+               "adatm_engine_update_from")
+
+    def fit_step(self):
+        f = C.c_double(0)
+        _check(lib().adatm_engine_fit_step(self._h, C.byref(f)), "adatm_engine_fit_step")
+        return f.value
+
+    def ttnorm(self):
+        v = C.c_double(0)
+        _check(lib().adatm_engine_ttnorm(self._h, C.byref(v)), "adatm_engine_ttnorm")
+        return v.value
+
+    def set_ttnorm(self, v):
+        _check(lib().adatm_engine_set_ttnorm(self._h, float(v)), "adatm_engine_set_ttnorm")
+
     def set_walkers(self, walkers):
         """Walkers per warp in the contraction source loop (1, 2, 4; 0 =
         the default for the rank)."""

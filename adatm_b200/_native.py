@@ -147,6 +147,11 @@ _SIGS = [
     ("adatm_engine_time_sweeps", C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
     ("adatm_engine_time_mttkrp", C.c_int, [C.c_void_p, u64, C.c_int, C.POINTER(C.c_float)]),
     ("adatm_engine_fit", C.c_int, [C.c_void_p, P_f64]),
+    ("adatm_engine_mttkrp_into", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("adatm_engine_update_from", C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    ("adatm_engine_fit_step", C.c_int, [C.c_void_p, P_f64]),
+    ("adatm_engine_ttnorm", C.c_int, [C.c_void_p, P_f64]),
+    ("adatm_engine_set_ttnorm", C.c_int, [C.c_void_p, C.c_double]),
     ("adatm_engine_mttkrp_bytes", C.c_int, [C.c_void_p, u64, P_f64]),
     ("adatm_engine_hot_rows", C.c_int, [C.c_void_p, u64, C.POINTER(C.c_int)]),
     ("adatm_engine_autotune", C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),

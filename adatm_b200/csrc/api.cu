@@ -1203,6 +1203,33 @@ int adatm_engine_fit(adatm_engine *e, double *fit) {
   return guarded([&] { *fit = e->eng->fit_host(); });
 }
 
+int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, float *dev_out) {
+  return guarded([&] {
+    if (!e || !dev_out) throw BadInput("adatm_engine_mttkrp_into: null argument");
+    if (mode >= (uint64_t)e->eng->nmodes()) throw BadInput("mode out of range");
+    e->eng->mttkrp_into((int)mode, dev_out);
+  });
+}
+
+int adatm_engine_update_from(adatm_engine *e, uint64_t mode, const float *dev_M) {
+  return guarded([&] {
+    if (!e || !dev_M) throw BadInput("adatm_engine_update_from: null argument");
+    e->eng->update_from((int)mode, dev_M);
+  });
+}
+
+int adatm_engine_fit_step(adatm_engine *e, double *fit) {
+  return guarded([&] { *fit = e->eng->fit_step(); });
+}
+
+int adatm_engine_ttnorm(adatm_engine *e, double *local) {
+  return guarded([&] { *local = e->eng->ttnorm_local(); });
+}
+
+int adatm_engine_set_ttnorm(adatm_engine *e, double global) {
+  return guarded([&] { e->eng->set_ttnorm(global); });
+}
+
 int adatm_engine_mttkrp_bytes(adatm_engine *e, uint64_t mode, double *bytes) {
   return guarded([&] {
     if (mode >= (uint64_t)e->eng->nmodes()) throw BadInput("mode out of range");

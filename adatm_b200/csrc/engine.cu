@@ -632,6 +632,47 @@ void Engine::sweep_eager() {
   fit(gs, w_, stream_);
 }
 
+void Engine::mttkrp_into(int mode, float *dev_out) {
+  mttkrp_as(mode, dev_out, sweep_type(mode));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void Engine::update_from(int mode, const float *dev_M) {
+  const int N = coo_->nmodes;
+  if (mode < 0 || mode >= N) throw BadInput("mode out of range");
+  GramSet gs;
+  for (int m = 0; m < kMaxModes; ++m) gs.G[m] = m < N ? G_[m].get() : nullptr;
+  gram_inverse(gs, mode, w_, stream_);
+  update_factor(dev_M, coo_->dims[mode], A_[mode].get(), Ab_[mode].get(), G_[mode].get(),
+                mode == N - 1, w_, stream_);
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
+double Engine::fit_step() {
+  const int N = coo_->nmodes;
+  GramSet gs;
+  for (int m = 0; m < kMaxModes; ++m) gs.G[m] = m < N ? G_[m].get() : nullptr;
+  fit(gs, w_, stream_);
+  return fit_host();
+}
+
+double Engine::ttnorm_local() {
+  if (!ttnorm_ready_) {
+    frob_sq(csf_[0]->vals64.get(), coo_->nnz, w_, stream_);
+    ttnorm_ready_ = true;
+  }
+  double v = 0;
+  ADATM_CUDA(cudaMemcpyAsync(&v, w_.scalars.get(), sizeof(double), cudaMemcpyDeviceToHost, stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+  return v;
+}
+
+void Engine::set_ttnorm(double v) {
+  ttnorm_local();  // keeps als_begin from recomputing it
+  ADATM_CUDA(cudaMemcpyAsync(w_.scalars.get(), &v, sizeof(double), cudaMemcpyHostToDevice, stream_));
+  ADATM_CUDA(cudaStreamSynchronize(stream_));
+}
+
 void Engine::capture_graph() {
   if (graph_exec_) return;
   // kernels set their shared-memory attributes on first use: run the

@@ -98,6 +98,22 @@ class Engine {
   float *mttkrp_buffer() { return M_.get(); }
   const float *memo_rows(int g, int deg) const { return memo_[g][deg].get(); }
 
+  // One shard of a tensor split across ranks (the nonzeros of some root
+  // slices; factors replicated): the sweep runs mode by mode with the sum of
+  // the ranks' MTTKRPs taken outside the engine between the two halves.
+  //   mttkrp_into(m, buf): this shard's MTTKRP of mode m into a device
+  //     buffer (dims[m] x ldr), finished when the call returns;
+  //   update_from(m, buf): the mode-m update (Gram inverse, A = M V^-1,
+  //     normalisation, Gram, the fit's inner product for the last mode)
+  //     from the summed MTTKRP, finished when the call returns;
+  //   fit_step(): the fit from the Grams, lambda and the inner product.
+  // ttnorm_local() / set_ttnorm(): this shard's ||X||^2 and the global one.
+  void mttkrp_into(int mode, float *dev_out);
+  void update_from(int mode, const float *dev_M);
+  double fit_step();
+  double ttnorm_local();
+  void set_ttnorm(double v);
+
   // CP-ALS
   void als_begin();                      // Grams, ||X||^2, iteration counter
   void sweep();                          // one ALS iteration (graph replay if captured)

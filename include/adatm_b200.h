@@ -254,6 +254,23 @@ int adatm_engine_als_begin(adatm_engine *e, int use_graph);
 int adatm_engine_time_sweeps(adatm_engine *e, int count, float *ms);
 int adatm_engine_time_mttkrp(adatm_engine *e, uint64_t mode, int count, float *ms);
 int adatm_engine_fit(adatm_engine *e, double *fit);
+
+/* One shard of a tensor split across ranks by root slices (each rank holds
+ * an engine on its nonzeros, same dims and plan; factors are replicated).
+ * A sweep runs mode by mode: adatm_engine_mttkrp_into writes this shard's
+ * MTTKRP of `mode` to a device buffer (dims[mode] x ldr floats, ldr = R
+ * rounded up to 4); the caller sums the ranks' buffers (an all-reduce);
+ * adatm_engine_update_from runs the mode's update from the summed buffer;
+ * after the last mode adatm_engine_fit_step gives the fit. ||X||^2 is the
+ * sum of the shards' adatm_engine_ttnorm values, set on every rank with
+ * adatm_engine_set_ttnorm. Calls return when their work is done. Start with
+ * adatm_engine_als_begin(e, 0). The reference's only collective is the fit's
+ * MPI all-reduce (adatm_cpd.c:147-157); this split adds the MTTKRP sum. */
+int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, float *dev_out);
+int adatm_engine_update_from(adatm_engine *e, uint64_t mode, const float *dev_M);
+int adatm_engine_fit_step(adatm_engine *e, double *fit);
+int adatm_engine_ttnorm(adatm_engine *e, double *local);
+int adatm_engine_set_ttnorm(adatm_engine *e, double global);
 /* Compulsory HBM bytes of the MTTKRP of `mode` as a sweep runs it. With BF16
  * rows, the tree that feeds the last mode (whose MTTKRP gives the fit's
  * inner product) still reads FP32 rows. */
