@@ -143,21 +143,6 @@ static int write_rows(const char *fname, const val_t *v, idx_t rows, idx_t cols)
   return 1;
 }
 
-static void print_groups(const group_properties *g, idx_t n_grp, idx_t nmodes) {
-  for (idx_t i = 0; i < n_grp; ++i) {
-    printf("  group %lu: memo_mode %lu begin_imten %lu n_imten %lu o_opt [", (unsigned long)i,
-           (unsigned long)g[i].memo_mode, (unsigned long)g[i].begin_imten,
-           (unsigned long)g[i].n_imten);
-    for (idx_t m = 0; m < nmodes; ++m) printf(m ? " %lu" : "%lu", (unsigned long)g[i].o_opt[m]);
-    printf("]\n");
-  }
-}
-
-static void print_idx(const idx_t *a, idx_t n, const char *name) {
-  printf("%s:", name);
-  for (idx_t i = 0; i < n; ++i) printf(" %lu", (unsigned long)a[i]);
-  printf("\n");
-}
 
 /* ------------------------------------------------------------------------ */
 
@@ -225,7 +210,7 @@ static int cmd_cpd(int argc, char **argv) {
   }
   printf("Optimal predicted grp_prop:\n");
   printf("n_grp: %lu\n", (unsigned long)n_grp);
-  print_groups(grp, n_grp, nmodes);
+  print_group_properties(grp, n_grp, nmodes, "Optimal grp_prop");
   idx_t n_csf = 0;
   splatt_csf *csf = csf_alloc_adaptive(tt, grp, n_grp, opts, &n_csf);
   if (csf == NULL) {
@@ -239,16 +224,20 @@ static int cmd_cpd(int argc, char **argv) {
   free_tns(tt);
   printf("** CSF **\n");
   printf("CSF-STORAGE: %zu bytes\n\n", csf_storage_adaptive(csf, n_csf, grp, (int)n_grp));
+  stats_csf_adaptive(csf, n_csf);
+  printf("\n");
   idx_t n_rcsf = 0;
   rcsf_seq_adaptive *rs = rcsf_alloc_adaptive(csf, nfactors, grp, n_grp, n_csf, opts, &n_rcsf);
   printf("n_rcsf: %lu\n", (unsigned long)n_rcsf);
   printf("** RCSF **\n");
-  printf("RCSF-STORAGE: %zu bytes\n\n", rcsf_storage_adaptive(rs, n_rcsf));
+  printf("RCSF-STORAGE: %zu bytes\n", rcsf_storage_adaptive(rs, n_rcsf));
+  stats_rcsf_adaptive(rs, n_rcsf);
+  printf("\n");
   fflush(stdout);
   idx_t use_csfs[SPLATT_MAX_NMODES], use_tags[SPLATT_MAX_NMODES];
   decide_use_csfs(nmodes, grp, (int)n_grp, n_csf, use_csfs, use_tags);
-  print_idx(use_csfs, nmodes, "use_csfs");
-  print_idx(use_tags, nmodes, "use_tags");
+  iprint_array(use_csfs, nmodes, "use_csfs");
+  iprint_array(use_tags, nmodes, "use_tags");
   splatt_kruskal k;
   const int ret = splatt_cpd_als_adaptive(csf, rs, n_csf, grp, n_grp, use_csfs, use_tags, nfactors,
                                           opts, &k);

@@ -855,12 +855,11 @@ void bench_adaptm(sptensor_t *const tt, matrix_t **mats, bench_opts const *const
     const uint64_t R = mats[0]->J;
     Plan p = plan_analytic(*coo, R, 1, nullptr, s.s);
     printf("Optimal predicted group properties:\nNumber of groups: %d\n", p.n_grp);
-    printf("====== Optimal grp_prop =======\n[memo_mode, begin_imten, n_imten, o_opt]\n");
-    for (int g = 0; g < p.n_grp; ++g) {
-      printf("%" PRIu64 ", %" PRIu64 ", %" PRIu64 ", \no_opt: \n", p.grp[g].memo_mode,
-             p.grp[g].begin_imten, p.grp[g].n_imten);
-      for (int l = 0; l < p.nmodes; ++l) printf(" %" PRIu64, p.grp[g].o_opt[l]);
-      printf("\n");
+    {
+      group_properties *gp = groups_to_c(p);
+      char title[] = "Optimal grp_prop";
+      print_group_properties(gp, (idx_t)p.n_grp, (idx_t)p.nmodes, title);
+      adatm_free_groups(gp, (idx_t)p.n_grp);
     }
     EngineOptions eo;
     Engine e(coo, {}, R, p, eo, s.s);
@@ -890,6 +889,59 @@ void bench_adaptm(sptensor_t *const tt, matrix_t **mats, bench_opts const *const
     cudaEventDestroy(b);
   });
   if (rc != SPLATT_SUCCESS) fprintf(stderr, "bench_adaptm: %s\n", g_last_error.c_str());
+}
+
+static void stats_one(splatt_csf const *ct) {
+  // p_stats_csf_mode (adatm_stats.c:19-49): one tile, never empty here
+  printf("nmodes: %" PRIu64 " nnz: %" PRIu64 "\n", ct->nmodes, ct->nnz);
+  printf("dims: %" PRIu64 "", ct->dims[0]);
+  for (idx_t m = 1; m < ct->nmodes; ++m) printf("x%" PRIu64 "", ct->dims[m]);
+  printf(" (%" PRIu64 "", ct->dim_perm[0]);
+  for (idx_t m = 1; m < ct->nmodes; ++m) printf("->%" PRIu64 "", ct->dim_perm[m]);
+  printf(")\n");
+  printf("ntiles: %" PRIu64 " tile dims: %" PRIu64 "", ct->ntiles, ct->tile_dims[0]);
+  for (idx_t m = 1; m < ct->nmodes; ++m) printf("x%" PRIu64 "", ct->tile_dims[m]);
+  idx_t empty = 0;
+  for (idx_t t = 0; t < ct->ntiles; ++t)
+    if (ct->pt[t].vals == nullptr) ++empty;
+  printf("  empty: %" PRIu64 " (%0.1f%%)\n", empty, 100. * (double)empty / (double)ct->ntiles);
+}
+
+void stats_csf_adaptive(splatt_csf const *const ct, idx_t const n_csf) {
+  for (idx_t g = 0; g < n_csf; ++g) {
+    printf("CSF-%" PRIu64 "\n", g);
+    stats_one(ct + g);
+  }
+}
+
+void stats_rcsf_adaptive(rcsf_seq_adaptive const *const seq_rcsfs, idx_t const n_rcsf) {
+  for (idx_t g = 0; g < n_rcsf; ++g) {
+    printf("vCSF Seq %" PRIu64 "\n", g);
+    for (idx_t i = 0; i < seq_rcsfs[g].n_imten; ++i) {
+      printf("   vCSF[%" PRIu64 "]:\n", i);
+      stats_one(seq_rcsfs[g].rcsfs + i);
+    }
+  }
+}
+
+void iprint_array(idx_t const *const array, idx_t const len, char const *const name) {
+  printf("%s: \n", name);
+  for (idx_t i = 0; i < len; ++i) printf(" %" PRIu64, array[i]);
+  printf("\n");
+  fflush(stdout);
+}
+
+void print_group_properties(group_properties *const grp_prop, idx_t const size, idx_t const nmodes,
+                            char *const name) {
+  printf("====== %s =======\n", name);
+  printf("[memo_mode, begin_imten, n_imten, o_opt]\n");
+  for (idx_t i = 0; i < size; ++i) {
+    printf("%" PRIu64 ", %" PRIu64 ", %" PRIu64 ", \n", grp_prop[i].memo_mode,
+           grp_prop[i].begin_imten, grp_prop[i].n_imten);
+    iprint_array(grp_prop[i].o_opt, nmodes, "o_opt");
+  }
+  printf("\n");
+  fflush(stdout);
 }
 
 int adatm_rcsf_pull(rcsf_seq_adaptive *rs_seq, idx_t n_rcsf) {

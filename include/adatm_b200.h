@@ -141,6 +141,18 @@ double cpd_als_iterate_adaptive(splatt_csf const *const tensors, rcsf_seq_adapti
  * opts->niters MTTKRP sequences and print per-mode seconds. */
 void bench_adaptm(sptensor_t *const tt, matrix_t **mats, bench_opts const *const opts);
 
+/* The reference's report lines, same text: stats_csf_adaptive prints every
+ * tree's order, nnz, dims, level order and tiles (adatm_stats.c:19-67),
+ * stats_rcsf_adaptive every memo tree of every sequence
+ * (adatm_stats.c:70-87), print_group_properties a group list
+ * (adatm_debug.c:58-72), iprint_array an index array (adatm_debug.c:5-15).
+ * Host only: they read the host views of the trees. */
+void stats_csf_adaptive(splatt_csf const *const ct, idx_t const n_csf);
+void stats_rcsf_adaptive(rcsf_seq_adaptive const *const seq_rcsfs, idx_t const n_rcsf);
+void print_group_properties(group_properties *const grp_prop, idx_t const size, idx_t const nmodes,
+                            char *const name);
+void iprint_array(idx_t const *const array, idx_t const len, char const *const name);
+
 /* Copy the device memo rows of rs_seq (all sequences, all trees) into their
  * host vals arrays. Not in the reference, whose memo rows live on the host. */
 int adatm_rcsf_pull(rcsf_seq_adaptive *rs_seq, idx_t n_rcsf);

@@ -94,3 +94,46 @@ def test_errors_are_reported_not_raised_in_c():
                                A.splatt_default_opts().ctypes.data_as(C.POINTER(C.c_double)))
     assert rc == A.SPLATT_ERROR_BADINPUT
     assert "not built by this library" in A._native.last_error()
+
+
+PRINT_WORKER = r"""
+import ctypes as C, sys
+sys.path.insert(0, {root!r})
+import numpy as np
+import adatm_b200 as A
+from adatm_b200 import _native as N
+L = A.lib()
+groups = [{{"memo_mode": 0, "begin_imten": 2, "n_imten": 1, "o_opt": [0, 1, 3, 2]}},
+          {{"memo_mode": 2, "begin_imten": 2, "n_imten": 1, "o_opt": [2, 3, 0, 1]}}]
+ga = A._GroupArray(groups, 4)
+L.print_group_properties.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_char_p]
+L.print_group_properties(C.cast(ga.arr, C.c_void_p), 2, 4, b"Optimal grp_prop")
+pt = N.CsfSparsity()
+pt.vals = (C.c_double * 1)(1.0)
+ct = N.SplattCsf(nnz=123, nmodes=4, which_tile=0, ntiles=1)
+for m, (d, p) in enumerate(zip([50, 40, 30, 20], [0, 1, 3, 2])):
+    ct.dims[m] = d; ct.dim_perm[m] = p; ct.tile_dims[m] = 1
+ct.pt = C.pointer(pt)
+L.stats_csf_adaptive.argtypes = [C.c_void_p, C.c_uint64]
+L.stats_csf_adaptive(C.cast(C.pointer(ct), C.c_void_p), 1)
+L.iprint_array.argtypes = [C.c_void_p, C.c_uint64, C.c_char_p]
+a = np.array([0, 0, 1, 1], dtype=np.uint64)
+L.iprint_array(a.ctypes.data_as(C.c_void_p), 4, b"use_csfs")
+"""
+
+
+def test_report_lines_have_the_reference_format():
+    """print_group_properties (adatm_debug.c:58-72), stats_csf_adaptive
+    (adatm_stats.c:19-67) and iprint_array (adatm_debug.c:5-15) print the
+    reference's text (host only, no GPU)."""
+    out = subprocess.run([__import__("sys").executable, "-c", PRINT_WORKER.format(root=ROOT)],
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    want = ("====== Optimal grp_prop =======\n"
+            "[memo_mode, begin_imten, n_imten, o_opt]\n"
+            "0, 2, 1, \no_opt: \n 0 1 3 2\n"
+            "2, 2, 1, \no_opt: \n 2 3 0 1\n\n"
+            "CSF-0\nnmodes: 4 nnz: 123\ndims: 50x40x30x20 (0->1->3->2)\n"
+            "ntiles: 1 tile dims: 1x1x1x1  empty: 0 (0.0%)\n"
+            "use_csfs: \n 0 0 1 1\n")
+    assert out.stdout == want, out.stdout
