@@ -256,7 +256,8 @@ class ReferenceRun:
         return 1e3 * seconds / n / self.fraction
 
     def describe(self, n):
-        src = "the reference's AdaTM C files" if self.kind == "reference" else "the oracle port"
+        src = (f"the reference's AdaTM C files (-O3 -march={self.O.ref_build_arch()})"
+               if self.kind == "reference" else "the oracle port")
         return (f"{n} CP-ALS sweeps of {src} (FP64, {self.threads} OpenMP threads) on a seeded "
                 f"random {self.fraction:.4f} of the nonzeros ({self.nnz} of them, same dims), "
                 f"time per sweep scaled by 1/{self.fraction:.4f}")

@@ -452,10 +452,30 @@ def ref_available() -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", "libadatm_ref.so"))
 
 
+def _host_has_avx512() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    fl = set(line.split(":", 1)[1].split())
+                    return {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"} <= fl
+    except OSError:
+        pass
+    return False
+
+
+def ref_build_arch() -> str:
+    """The build of the reference's code this host loads: x86-64-v4 (AVX-512)
+    where the CPU has it and that build exists, else x86-64-v3."""
+    v4 = os.path.join(HERE, "_ref", "libadatm_ref_v4.so")
+    return "x86-64-v4" if _host_has_avx512() and os.path.exists(v4) else "x86-64-v3"
+
+
 def ref():
     global _ref
     if _ref is None:
-        L = C.CDLL(os.path.join(HERE, "_ref", "libadatm_ref.so"))
+        name = "libadatm_ref_v4.so" if ref_build_arch() == "x86-64-v4" else "libadatm_ref.so"
+        L = C.CDLL(os.path.join(HERE, "_ref", name))
         L.ref_plan.argtypes = [C.c_int, u64, P_u64, P_u64, P_f64, u64, P_u64]
         L.ref_plan.restype = u64
         L.ref_build.argtypes = [C.c_int, u64, P_u64, P_u64, P_f64, u64, P_u64, C.c_int]
