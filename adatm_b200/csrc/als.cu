@@ -169,9 +169,9 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
 // Row pass of a mode update (or of a plain Gram). Each block takes row
 // groups of 256 / LANES rows; the rows (A = M V^-1, or M itself) are staged
 // in shared memory and their Gram X^T X is taken on the tensor cores: G is
-// tiled in 16 x 8 tiles spread over the block's 8 warps, each tile a chain of
-// m16n8k8 TF32 MMAs over the group's rows with FP32 accumulation, added to
-// FP64 per-thread sums after every group. FP32 rows split into a TF32 big
+// tiled in 16 x 8 tiles spread over the block's 8 warps; every 8 rows of a
+// tile are one m16n8k8 TF32 MMA step with FP32 accumulation, added to FP64
+// per-thread sums after the step. FP32 rows split into a TF32 big
 // part and a TF32 remainder, and big*big + big*rem + rem*big keeps the
 // products to ~2^-22 (split = 1); BF16-valued rows are exact in TF32 and
 // take one product.
@@ -248,9 +248,9 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
       const int tile = warp + 8 * tt;
       const int i0 = (tile / TN) * 16, j0 = (tile % TN) * 8;
       if (tile < NT && i0 < R && j0 < R) {
-        float c[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int k0 = 0; k0 < GROUPS; k0 += 8) {
+          float c[4] = {0.f, 0.f, 0.f, 0.f};
           // A = X^T (rows i0.., the group's rows as k), B = X (columns j0..)
           const float *x0 = rowbuf + (k0 + tig) * RS, *x1 = rowbuf + (k0 + tig + 4) * RS;
           const float av[4] = {x0[i0 + gid], x0[i0 + gid + 8], x1[i0 + gid], x1[i0 + gid + 8]};
@@ -270,9 +270,9 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
             mma_tf32(c, ab, bs);
             mma_tf32(c, as, bb);
           }
-        }
 #pragma unroll
-        for (int q = 0; q < 4; ++q) gacc[tt][q] += (double)c[q];
+          for (int q = 0; q < 4; ++q) gacc[tt][q] += (double)c[q];
+        }
       }
     }
     if (tid < R)

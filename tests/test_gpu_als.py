@@ -91,7 +91,8 @@ def test_gram_device_entry_point(gpu, rows, R):
     G = torch.zeros(R, R, device="cuda", dtype=torch.float64)
     A.gram_device(x.data_ptr(), rows, R, ldr, G.data_ptr())
     ref = x[:, :R].double().T @ x[:, :R].double()
-    assert torch.allclose(G, ref, rtol=1e-10, atol=1e-9)
+    # TF32 tensor-core tiles (three-term split) with FP32 sums per 8 rows
+    assert torch.allclose(G, ref, rtol=1e-6, atol=1e-6 * float(ref.abs().max()))
 
 
 def test_bf16_sweep_fit_tracks_fp32(gpu):
