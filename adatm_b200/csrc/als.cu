@@ -633,33 +633,34 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoallocDoubles];
 namespace {
 
 struct NoallocSlot {
-  std::once_flag once;
+  std::mutex mu;
+  bool ready = false;
   double *ptr = nullptr;
-  cudaError_t err = cudaSuccess;
 };
 NoallocSlot g_noalloc_slots[kNoallocMaxDevices];
 
-// Device address of the scratch on the current device (resolved once).
+// Device address of the scratch on the current device, resolved on the
+// first successful call and kept; a failed set-up is not kept, so a later
+// call tries again. cudaDeviceReset unloads the module that holds the
+// scratch: the kept address is then stale, so a process must not call the
+// entry point again after resetting the device.
 double *noalloc_scratch() {
   int dev = 0;
   ADATM_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNoallocMaxDevices) throw BadInput("device ordinal above the scratch table");
   NoallocSlot &slot = g_noalloc_slots[dev];
-  std::call_once(slot.once, [&] {
+  std::lock_guard<std::mutex> lk(slot.mu);
+  if (!slot.ready) {
     void *p = nullptr;
-    slot.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (slot.err == cudaSuccess) {
-      try {
-        set_attributes();
-      } catch (const CudaError &) {
-        slot.err = cudaGetLastError();
-        if (slot.err == cudaSuccess) slot.err = cudaErrorUnknown;
-      }
+    const cudaError_t err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (err != cudaSuccess) {
+      cudaGetLastError();
+      throw CudaError(std::string("scratch set-up failed: ") + cudaGetErrorString(err));
     }
+    set_attributes();
     slot.ptr = static_cast<double *>(p);
-  });
-  if (slot.err != cudaSuccess)
-    throw CudaError(std::string("scratch set-up failed: ") + cudaGetErrorString(slot.err));
+    slot.ready = true;
+  }
   return slot.ptr;
 }
 

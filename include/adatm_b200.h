@@ -393,7 +393,8 @@ int adatm_gram(const float *A, uint64_t rows, int R, int ldr, double *G);
  * Runs on `stream` (a cudaStream_t; NULL = the legacy default stream) and
  * returns after it completes. Calls that overlap in time on one device race
  * on the shared array. The first call on a device resolves the array's
- * address; make it once before any stream capture. */
+ * address; make it once before any stream capture. After cudaDeviceReset
+ * the resolved address is stale: do not call it again in that process. */
 int adatm_gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, void *stream);
 
 /* Number of kernel launches of one sweep and of one MTTKRP of `mode`. */

@@ -34,6 +34,33 @@ def test_gram_noalloc_matches_gram(gpu, rows, R):
         assert torch.allclose(G, ref, rtol=1e-12, atol=1e-12 * float(ref.abs().max()))
 
 
+def test_gram_noalloc_allocates_nothing(gpu):
+    """After a first call (set-up), further calls leave the device's free
+    memory unchanged, and they still succeed while a torch tensor holds
+    nearly all of it."""
+    import torch
+    lib = A.lib()
+    x, ldr = _rows(torch, 20000, 32, 5)
+    G = torch.zeros(32, 32, device="cuda", dtype=torch.float64)
+    call = lambda: lib.adatm_gram_noalloc(C.c_void_p(x.data_ptr()), 20000, 32, ldr,
+                                          C.c_void_p(G.data_ptr()), None)
+    assert call() == A.SPLATT_SUCCESS, A._native.last_error()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        assert call() == A.SPLATT_SUCCESS
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    ref = G.clone()
+    hog = torch.empty(max(0, free0 - (256 << 20)), dtype=torch.uint8, device="cuda")
+    try:
+        assert call() == A.SPLATT_SUCCESS, A._native.last_error()
+        assert torch.equal(G, ref)
+    finally:
+        del hog
+        torch.cuda.empty_cache()
+
+
 def test_gram_noalloc_rejects_rank_above_scratch(gpu):
     import torch
     lib = A.lib()
