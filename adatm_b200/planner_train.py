@@ -77,11 +77,25 @@ def measure_tensor(t, sweeps=5, R=RANK):
     return X, nbytes, cands, ms, chosen
 
 
+def _save(path, rows, labels, tid, cidx, analytic, specs):
+    np.savez(path, X=np.array(rows, dtype=np.float32).reshape(-1, A.PLAN_FEATURES),
+             y=np.array(labels, dtype=np.float32), tensor=np.array(tid, dtype=np.int64),
+             cand=np.array(cidx, dtype=np.int64), analytic=np.array(analytic, dtype=np.int64),
+             specs=np.array(specs))
+
+
 def make(args):
+    import time
     A.lib().adatm_set_device(0)
     rows, labels, tid, cidx, analytic, specs = [], [], [], [], [], []
     ranks = [int(r) for r in args.ranks.split(",")]
+    t_start = time.time()
     for k in range(args.tensors):
+        if args.time_limit and time.time() - t_start > args.time_limit:
+            print(f"time limit reached after {k} tensors", flush=True)
+            break
+        if k and args.checkpoint and k % args.checkpoint == 0:
+            _save(args.out, rows, labels, tid, cidx, analytic, specs)
         seed = args.seed0 + k
         N, dims, nnz, alpha, R = draw_tensor_spec(seed, args.max_nnz, args.min_nnz, args.min_order,
                                                   ranks)
@@ -99,9 +113,7 @@ def make(args):
                                  "R": R}))
         print(f"tensor {k} N={N} R={R} nnz={nnz} cands={len(cands)} ms={np.round(ms, 3).tolist()} "
               f"analytic={chosen}", flush=True)
-    np.savez(args.out, X=np.array(rows, dtype=np.float32), y=np.array(labels, dtype=np.float32),
-             tensor=np.array(tid), cand=np.array(cidx), analytic=np.array(analytic),
-             specs=np.array(specs))
+    _save(args.out, rows, labels, tid, cidx, analytic, specs)
 
 
 def regrets(y, tensor, cand, analytic, pred, ids):
@@ -172,7 +184,7 @@ def evaluate(args):
     A.lib().adatm_set_device(0)
     model = A.PlanModel.load(args.model)
     if args.big:
-        t = A.Tensor.generate(BIG_DIMS, BIG_NNZ, alpha=BIG_ALPHA, seed=2026)
+        t = A.Tensor.generate(BIG_DIMS, BIG_NNZ, alpha=BIG_ALPHA, seed=args.big_seed)
     else:
         N, dims, nnz, alpha, _ = draw_tensor_spec(args.seed, args.max_nnz)
         t = A.Tensor.generate(dims, nnz, alpha=alpha, seed=args.seed)
@@ -200,6 +212,8 @@ def main():
     m.add_argument("--ranks", default=str(RANK))
     m.add_argument("--sweeps", type=int, default=5)
     m.add_argument("--out", required=True)
+    m.add_argument("--time-limit", type=float, default=0, help="stop after this many seconds")
+    m.add_argument("--checkpoint", type=int, default=100, help="save every this many tensors")
     t = sub.add_parser("train")
     t.add_argument("--data", action="append", required=True)
     t.add_argument("--model", default=DEFAULT_MODEL)
@@ -210,6 +224,7 @@ def main():
     e = sub.add_parser("eval")
     e.add_argument("--model", default=DEFAULT_MODEL)
     e.add_argument("--big", action="store_true")
+    e.add_argument("--big-seed", type=int, default=0, help="seed of the held-out 6th-order tensor")
     e.add_argument("--seed", type=int, default=99999)
     e.add_argument("--max-nnz", type=float, default=4e6)
     e.add_argument("--sweeps", type=int, default=5)
