@@ -764,7 +764,7 @@ class Engine:
 
     # one shard of a tensor split across ranks (adatm_b200.shard)
     def mttkrp_into(self, mode, dev_ptr):
-        """This shard's MTTKRP of `mode` into a device buffer (dims[mode] x ldr FP32)."""
+        """This shard's MTTKRP of `mode` into a device buffer (dims[mode] x ldr FP64)."""
         _check(lib().adatm_engine_mttkrp_into(self._h, mode, C.c_void_p(dev_ptr)),
                "adatm_engine_mttkrp_into")
 

@@ -140,7 +140,8 @@ __global__ void __launch_bounds__(256) k_gram_inverse(GramSet g, int nmodes, int
 // ---------------------------------------------------------------------------
 struct UpdArgs {
   int split;           // Gram products as 3 TF32 terms (FP32 rows) or 1 (BF16-valued rows)
-  const float *M;
+  const double *Md;    // MTTKRP rows (FP64) of an update, or nullptr
+  const float *M;      // rows whose Gram alone is wanted (vinv == nullptr)
   const double *vinv;  // R x R fp64, or nullptr for identity
   float *A;           // output rows (may alias M when vinv == nullptr)
   uint64_t rows;
@@ -211,8 +212,23 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
        row0 += (uint64_t)gridDim.x * GROUPS) {
     const uint64_t i = row0 + g;
     const bool valid = i < a.rows;
-    float4 m = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (valid && act) m = *reinterpret_cast<const float4 *>(a.M + i * a.ldr + col);
+    double md[4] = {0.0, 0.0, 0.0, 0.0};
+    if (valid && act) {
+      if (a.Md) {
+        const double2 lo = *reinterpret_cast<const double2 *>(a.Md + i * a.ldr + col);
+        const double2 hi = *reinterpret_cast<const double2 *>(a.Md + i * a.ldr + col + 2);
+        md[0] = lo.x;
+        md[1] = lo.y;
+        md[2] = hi.x;
+        md[3] = hi.y;
+      } else {
+        const float4 f = *reinterpret_cast<const float4 *>(a.M + i * a.ldr + col);
+        md[0] = f.x;
+        md[1] = f.y;
+        md[2] = f.z;
+        md[3] = f.w;
+      }
+    }
     float4 o;
     if (a.vinv) {
       // A = M V^-1 with V^-1 and the sums in FP64: V (the Hadamard of the
@@ -220,10 +236,8 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
       // inverse's large entries of both signs lose the fit's digits
       double o0 = 0.0, o1 = 0.0, o2 = 0.0, o3 = 0.0;
       for (int kk = 0; kk < kq; ++kk) {
-        const double m4[4] = {(double)__shfl_sync(gmask, m.x, kk, LANES),
-                              (double)__shfl_sync(gmask, m.y, kk, LANES),
-                              (double)__shfl_sync(gmask, m.z, kk, LANES),
-                              (double)__shfl_sync(gmask, m.w, kk, LANES)};
+        const double m4[4] = {__shfl_sync(gmask, md[0], kk, LANES), __shfl_sync(gmask, md[1], kk, LANES),
+                              __shfl_sync(gmask, md[2], kk, LANES), __shfl_sync(gmask, md[3], kk, LANES)};
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           const double *vr = vinv + (4 * kk + q) * RMAX + col;
@@ -238,7 +252,7 @@ __global__ void __launch_bounds__(256) k_update(UpdArgs a) {
       o = make_float4((float)o0, (float)o1, (float)o2, (float)o3);
       if (valid && act) *reinterpret_cast<float4 *>(a.A + i * a.ldr + col) = o;
     } else {
-      o = m;
+      o = make_float4((float)md[0], (float)md[1], (float)md[2], (float)md[3]);
     }
     *reinterpret_cast<float4 *>(rowbuf + g * RS + col) =
         valid ? o : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -350,7 +364,7 @@ int finalize_blocks(int R) { return (R * R + kFinEntries - 1) / kFinEntries; }
 
 // A /= lambda (fp32), bf16 copy, optional partial <A, M> per column.
 template <int LANES>
-__global__ void __launch_bounds__(256) k_scale(float *A, __nv_bfloat16 *Ab, const float *M,
+__global__ void __launch_bounds__(256) k_scale(float *A, __nv_bfloat16 *Ab, const double *M,
                                                uint64_t rows, int R, int ldr, const double *lam,
                                                double *part_inner) {
   constexpr int GROUPS = 256 / LANES;
@@ -386,11 +400,12 @@ __global__ void __launch_bounds__(256) k_scale(float *A, __nv_bfloat16 *Ab, cons
     }
     *reinterpret_cast<float4 *>(A + i * ldr + col) = v;
     if (part_inner) {
-      const float4 m = *reinterpret_cast<const float4 *>(M + i * ldr + col);
-      in0 += (double)v.x * m.x;
-      in1 += (double)v.y * m.y;
-      in2 += (double)v.z * m.z;
-      in3 += (double)v.w * m.w;
+      const double2 lo = *reinterpret_cast<const double2 *>(M + i * ldr + col);
+      const double2 hi = *reinterpret_cast<const double2 *>(M + i * ldr + col + 2);
+      in0 += (double)v.x * lo.x;
+      in1 += (double)v.y * lo.y;
+      in2 += (double)v.z * hi.x;
+      in3 += (double)v.w * hi.y;
     }
   }
   if (part_inner) {
@@ -536,6 +551,7 @@ void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, 
           bool bf16_rows) {
   UpdArgs u;
   u.split = bf16_rows ? 0 : 1;
+  u.Md = nullptr;
   u.M = A;
   u.vinv = nullptr;
   u.A = nullptr;
@@ -567,11 +583,12 @@ void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s) {
   ADATM_LAUNCH();
 }
 
-void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
+void update_factor(const double *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
                    bool inner, AlsWork &w, cudaStream_t s) {
   UpdArgs u;
   u.split = 1;
-  u.M = M;
+  u.Md = M;
+  u.M = nullptr;
   u.vinv = w.vinv64.get();
   u.A = A;
   u.rows = rows;
@@ -677,6 +694,7 @@ void gram_noalloc(const float *A, uint64_t rows, int R, int ldr, double *G, cuda
   double *scratch = noalloc_scratch();
   UpdArgs u;
   u.split = 1;
+  u.Md = nullptr;
   u.M = A;
   u.vinv = nullptr;
   u.A = nullptr;

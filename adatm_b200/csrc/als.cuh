@@ -41,12 +41,12 @@ void gram(const float *A, uint64_t rows, int R, int ldr, double *G, AlsWork &w, 
 void frob_sq(const double *vals, uint64_t n, AlsWork &w, cudaStream_t s);
 // V = Hadamard of all G[n], n != mode; write V^-1 (fp64).
 void gram_inverse(const GramSet &g, int mode, AlsWork &w, cudaStream_t s);
-// A = normalize(M * V^-1); updates lambda (2-norm on the first iteration,
+// A = normalize(M * V^-1) (M: the FP64 MTTKRP rows); updates lambda (2-norm on the first iteration,
 // max-norm floored at 1 afterwards), G_mode and, when `inner` is set, the
 // partial inner products <A, M> of the fit. A is fp32; with a bf16 copy (Ab
 // non-null) the rows are rounded to bf16 in both copies and G_mode is taken
 // from the rounded rows.
-void update_factor(const float *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
+void update_factor(const double *M, uint64_t rows, float *A, __nv_bfloat16 *Ab, double *G_mode,
                    bool inner, AlsWork &w, cudaStream_t s);
 // fit = 1 - sqrt(||X||^2 + ||Z||^2 - 2<X,Z>) / ||X||, stored in
 // w.scalars[1] and w.fit_trace[iter]; advances w.iter.

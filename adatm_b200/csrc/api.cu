@@ -371,6 +371,19 @@ std::shared_ptr<DevCoo> coo_of(sptensor_t *tt, cudaStream_t s) {
   return upload_coo((int)tt->nmodes, tt->nnz, tt->dims, tt->ind, tt->vals, s);
 }
 
+template <typename T>
+void pull_rows(Engine &e, const T *src, uint64_t rows, double *out) {
+  const int ldr = e.ldr();
+  const uint64_t R = e.rank();
+  std::vector<T> buf((size_t)rows * ldr);
+  if (rows)
+    ADATM_CUDA(cudaMemcpyAsync(buf.data(), src, buf.size() * sizeof(T), cudaMemcpyDeviceToHost,
+                               e.stream()));
+  ADATM_CUDA(cudaStreamSynchronize(e.stream()));
+  for (uint64_t i = 0; i < rows; ++i)
+    for (uint64_t r = 0; r < R; ++r) out[i * R + r] = buf[i * ldr + r];
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -551,8 +564,8 @@ int splatt_mttkrp(splatt_idx_t const mode, splatt_idx_t const ncolumns,
     e.set_factors(matrices);
     e.mttkrp_direct((int)mode, e.mttkrp_buffer());
     const uint64_t I = e.dims()[mode];
-    std::vector<float> buf((size_t)I * e.ldr());
-    ADATM_CUDA(cudaMemcpyAsync(buf.data(), e.mttkrp_buffer(), buf.size() * sizeof(float),
+    std::vector<double> buf((size_t)I * e.ldr());
+    ADATM_CUDA(cudaMemcpyAsync(buf.data(), e.mttkrp_buffer(), buf.size() * sizeof(double),
                                cudaMemcpyDeviceToHost, e.stream()));
     ADATM_CUDA(cudaStreamSynchronize(e.stream()));
     for (uint64_t i = 0; i < I; ++i)
@@ -790,8 +803,8 @@ void mttkrp_csf_adaptive(splatt_csf const *const tensors, rcsf_seq_adaptive cons
     e.set_factors(fm);
     e.mttkrp_with((int)mode, (int)use_csf, (int)use_tag, e.mttkrp_buffer());
     const uint64_t I = e.dims()[mode];
-    std::vector<float> buf((size_t)I * e.ldr());
-    ADATM_CUDA(cudaMemcpyAsync(buf.data(), e.mttkrp_buffer(), buf.size() * sizeof(float),
+    std::vector<double> buf((size_t)I * e.ldr());
+    ADATM_CUDA(cudaMemcpyAsync(buf.data(), e.mttkrp_buffer(), buf.size() * sizeof(double),
                                cudaMemcpyDeviceToHost, e.stream()));
     ADATM_CUDA(cudaStreamSynchronize(e.stream()));
     matrix_t *M = mats[SPLATT_MAX_NMODES];
@@ -1149,17 +1162,6 @@ int adatm_engine_get_factors(adatm_engine *e, double *const *mats, double *lambd
   });
 }
 
-static void pull_rows(Engine &e, const float *src, uint64_t rows, double *out) {
-  const int ldr = e.ldr();
-  const uint64_t R = e.rank();
-  std::vector<float> buf((size_t)rows * ldr);
-  if (rows)
-    ADATM_CUDA(cudaMemcpyAsync(buf.data(), src, buf.size() * sizeof(float), cudaMemcpyDeviceToHost,
-                               e.stream()));
-  ADATM_CUDA(cudaStreamSynchronize(e.stream()));
-  for (uint64_t i = 0; i < rows; ++i)
-    for (uint64_t r = 0; r < R; ++r) out[i * R + r] = buf[i * ldr + r];
-}
 
 int adatm_engine_mttkrp(adatm_engine *e, uint64_t mode, double *out) {
   return guarded([&] {
@@ -1255,7 +1257,7 @@ int adatm_engine_fit(adatm_engine *e, double *fit) {
   return guarded([&] { *fit = e->eng->fit_host(); });
 }
 
-int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, float *dev_out) {
+int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, double *dev_out) {
   return guarded([&] {
     if (!e || !dev_out) throw BadInput("adatm_engine_mttkrp_into: null argument");
     if (mode >= (uint64_t)e->eng->nmodes()) throw BadInput("mode out of range");
@@ -1263,7 +1265,7 @@ int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, float *dev_out) {
   });
 }
 
-int adatm_engine_update_from(adatm_engine *e, uint64_t mode, const float *dev_M) {
+int adatm_engine_update_from(adatm_engine *e, uint64_t mode, const double *dev_M) {
   return guarded([&] {
     if (!e || !dev_M) throw BadInput("adatm_engine_update_from: null argument");
     e->eng->update_from((int)mode, dev_M);

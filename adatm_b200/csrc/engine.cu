@@ -434,7 +434,7 @@ void Engine::set_use(const uint64_t *use_csfs, const uint64_t *use_tags) {
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Engine::mttkrp_with(int mode, int tree, int tag, float *out) {
+void Engine::mttkrp_with(int mode, int tree, int tag, double *out) {
   check_use(mode, tree, tag);
   const TreeWalk *w = nullptr;
   if ((int)plan_.use_csfs[mode] == tree && (int)plan_.use_tags[mode] == tag) {
@@ -444,7 +444,7 @@ void Engine::mttkrp_with(int mode, int tree, int tag, float *out) {
     if (!slot) slot = make_walk(mode, tree, tag);
     w = slot.get();
   }
-  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
+  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(double), stream_));
   walk_launch(*w, level_factors(tree, opt_.factor_type), opt_.factor_type, out, stream_);
 }
 
@@ -458,12 +458,12 @@ LevelFactors Engine::level_factors(int g, FactorType ft) const {
   return f;
 }
 
-void Engine::mttkrp_as(int mode, float *out, FactorType ft) {
-  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
+void Engine::mttkrp_as(int mode, double *out, FactorType ft) {
+  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(double), stream_));
   walk_launch(*walk_[mode], level_factors((int)plan_.use_csfs[mode], ft), ft, out, stream_);
 }
 
-void Engine::mttkrp(int mode, float *out) { mttkrp_as(mode, out, opt_.factor_type); }
+void Engine::mttkrp(int mode, double *out) { mttkrp_as(mode, out, opt_.factor_type); }
 
 FactorType Engine::sweep_type(int mode) const {
   // With BF16 factors every factor value is BF16-representable (the update
@@ -474,8 +474,8 @@ FactorType Engine::sweep_type(int mode) const {
   return opt_.factor_type;
 }
 
-void Engine::mttkrp_direct(int mode, float *out) {
-  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(float), stream_));
+void Engine::mttkrp_direct(int mode, double *out) {
+  ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(double), stream_));
   walk_launch(*direct_[mode], level_factors((int)plan_.use_csfs[mode], opt_.factor_type),
               opt_.factor_type, out, stream_);
 }
@@ -632,12 +632,12 @@ void Engine::sweep_eager() {
   fit(gs, w_, stream_);
 }
 
-void Engine::mttkrp_into(int mode, float *dev_out) {
+void Engine::mttkrp_into(int mode, double *dev_out) {
   mttkrp_as(mode, dev_out, sweep_type(mode));
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
 
-void Engine::update_from(int mode, const float *dev_M) {
+void Engine::update_from(int mode, const double *dev_M) {
   const int N = coo_->nmodes;
   if (mode < 0 || mode >= N) throw BadInput("mode out of range");
   GramSet gs;

@@ -68,22 +68,22 @@ class Engine {
   void get_normalized(double *const *host, double *lambda);
   float *factor(int m) { return A_[m].get(); }
 
-  // MTTKRP of `mode` following the plan (tags 0/1/2) into out (dims x ldr,
-  // zeroed here). Memo reuse (tag 1) expects the group's memo root to have
+  // MTTKRP of `mode` following the plan (tags 0/1/2) into out (dims x ldr
+  // FP64, zeroed here). Memo reuse (tag 1) expects the group's memo root to have
   // run on the current factors of the memoized levels.
-  void mttkrp(int mode, float *out);
+  void mttkrp(int mode, double *out);
   // same, with the factor rows read in the given precision
-  void mttkrp_as(int mode, float *out, FactorType ft);
+  void mttkrp_as(int mode, double *out, FactorType ft);
   // Row type of mode `mode`'s MTTKRP inside a sweep.
   FactorType sweep_type(int mode) const;
   // MTTKRP of `mode` recomputed on its group's tree without memo rows.
-  void mttkrp_direct(int mode, float *out);
+  void mttkrp_direct(int mode, double *out);
   // MTTKRP of `mode` the way a reference caller names it: on tree `tree`
   // with tag 0 (root MTTKRP; it stores the tree's memo rows when its group
   // memoizes), 1 (reuse of the tree's memo rows) or 2 (recompute from the
   // leaves), as mttkrp_csf_adaptive dispatches (mttkrp.c:2037-2090). The
   // walk is built on first use and kept.
-  void mttkrp_with(int mode, int tree, int tag, float *out);
+  void mttkrp_with(int mode, int tree, int tag, double *out);
   // Whether (mode, tree, tag) is a valid request on this plan's trees:
   // throws BadInput naming the problem (tag 0 on a mode that is not the
   // tree's root, tag 2 on the root, tag 1 on a tree without memo rows or
@@ -95,21 +95,21 @@ class Engine {
   // mode of the sweep, which writes the memo rows it reads. Rebuilds the
   // walks and drops a captured sweep when they change.
   void set_use(const uint64_t *use_csfs, const uint64_t *use_tags);
-  float *mttkrp_buffer() { return M_.get(); }
+  double *mttkrp_buffer() { return M_.get(); }
   const float *memo_rows(int g, int deg) const { return memo_[g][deg].get(); }
 
   // One shard of a tensor split across ranks (the nonzeros of some root
   // slices; factors replicated): the sweep runs mode by mode with the sum of
   // the ranks' MTTKRPs taken outside the engine between the two halves.
   //   mttkrp_into(m, buf): this shard's MTTKRP of mode m into a device
-  //     buffer (dims[m] x ldr), finished when the call returns;
+  //     buffer (dims[m] x ldr FP64), finished when the call returns;
   //   update_from(m, buf): the mode-m update (Gram inverse, A = M V^-1,
   //     normalisation, Gram, the fit's inner product for the last mode)
   //     from the summed MTTKRP, finished when the call returns;
   //   fit_step(): the fit from the Grams, lambda and the inner product.
   // ttnorm_local() / set_ttnorm(): this shard's ||X||^2 and the global one.
-  void mttkrp_into(int mode, float *dev_out);
-  void update_from(int mode, const float *dev_M);
+  void mttkrp_into(int mode, double *dev_out);
+  void update_from(int mode, const double *dev_M);
   double fit_step();
   double ttnorm_local();
   void set_ttnorm(double v);
@@ -167,7 +167,7 @@ class Engine {
   DevBuf<float> A_[kMaxModes];
   DevBuf<__nv_bfloat16> Ab_[kMaxModes];
   DevBuf<double> G_[kMaxModes];
-  DevBuf<float> M_;
+  DevBuf<double> M_;
   AlsWork w_;
   bool ttnorm_ready_ = false;    // ||X||^2 computed (the tensor never changes)
   float *staging_ = nullptr;     // pinned host rows for factor transfers

@@ -23,7 +23,7 @@ struct WalkArgs {
   const void *U_src;           // factor rows of the source level
   const void *U[kMaxModes];
   float *store[kMaxModes];
-  float *out;
+  double *out;                 // MTTKRP output rows (FP64 sums)
   const uint32_t *sched;
   uint32_t *counter;           // chunks claimed so far (zeroed before each launch)
   const uint8_t *hot_slot;     // scatter: slot of an output row summed per block, 0xFF = none
@@ -192,6 +192,33 @@ __device__ __forceinline__ void red_rows(float *base, uint64_t row, int ldr, int
   } else {
     atomicAdd(reinterpret_cast<float4 *>(p), make_float4(v.x[0], v.x[1], v.x[2], v.x[3]));
   }
+}
+
+// FP64 output rows: the MTTKRP sums of a row can come from millions of
+// units (a skewed slice), and FP32 sums of that many partials lose several
+// digits; outputs are stored and added in FP64.
+template <int V>
+__device__ __forceinline__ void st_out(double *base, uint64_t row, int ldr, int col, const fv<V> &v,
+                                       bool act) {
+  if (!act) return;
+  double *p = base + row * (uint64_t)ldr + col;
+  if constexpr (V == 1) {
+    *p = v.x[0];
+  } else if constexpr (V == 2) {
+    *reinterpret_cast<double2 *>(p) = make_double2(v.x[0], v.x[1]);
+  } else {
+    *reinterpret_cast<double2 *>(p) = make_double2(v.x[0], v.x[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v.x[2], v.x[3]);
+  }
+}
+
+template <int V>
+__device__ __forceinline__ void red_out(double *base, uint64_t row, int ldr, int col, const fv<V> &v,
+                                        bool act) {
+  if (!act) return;
+  double *p = base + row * (uint64_t)ldr + col;
+#pragma unroll
+  for (int i = 0; i < V; ++i) atomicAdd(p + i, (double)v.x[i]);
 }
 
 // Factor-row gathers through a per-lane base pointer (the lane's first
@@ -531,11 +558,11 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
             if (a.out == nullptr) {
               // deterministic d > 0: the level-d sums went to a store row
             } else if (d == 0) {
-              if (!(i == 0 && pfirst)) st_rows<V>(a.out, orow, a.ldr, col, val, act);
+              if (!(i == 0 && pfirst)) st_out<V>(a.out, orow, a.ldr, col, val, act);
               else if (a.span) st_rows<V>(span_row(a, chunk_id, 0, 0), 0, 0, col, val, act);
-              else red_rows<V>(a.out, orow, a.ldr, col, val, act);
+              else red_out<V>(a.out, orow, a.ldr, col, val, act);
             } else {
-              red_rows<V>(a.out, orow, a.ldr, col, fv_mul(val, pre[(d - 1) * 32 + lane]), act);
+              red_out<V>(a.out, orow, a.ldr, col, fv_mul(val, pre[(d - 1) * 32 + lane]), act);
               const uint32_t ci = __shfl_sync(~0u, icd, i);
               if (ci >= 1u) nodeL = advance_prefix<V, FT>(a, pre, nodeL, d - (int)ci, d, col, act, lane);
             }
@@ -571,8 +598,8 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
           st_rows<V>(span_row(a, chunk_id, 0, 1), 0, 0, col, val, act);
         } else {
           const uint32_t orow = __ldg(a.fids[d] + node);
-          red_rows<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
-                      act);
+          red_out<V>(a.out, orow, a.ldr, col, d == 0 ? val : fv_mul(val, pre[(d - 1) * 32 + lane]),
+                     act);
         }
       }
     }
@@ -648,24 +675,28 @@ __global__ void __launch_bounds__(256, HOT ? 3 : 1) k_scatter(const __grid_const
   // hot output rows: summed by the block in shared memory, added to the
   // output once at the end (their atomics would otherwise queue on a few L2
   // lines); the grid is then resident and warps stride over the chunks
-  float *hacc = HOT ? reinterpret_cast<float *>(walk_raw + kWarps * scatter_warp_bytes(a.ldr)) : nullptr;
+  double *hacc = HOT ? reinterpret_cast<double *>(walk_raw + kWarps * scatter_warp_bytes(a.ldr)) : nullptr;
   if constexpr (HOT) {
-    for (int i = threadIdx.x; i < a.nhot * a.ldr; i += blockDim.x) hacc[i] = 0.f;
+    for (int i = threadIdx.x; i < a.nhot * a.ldr; i += blockDim.x) hacc[i] = 0.0;
     __syncthreads();
   }
   auto emit = [&](uint32_t row, const float4 &x) {
     if constexpr (HOT) {
       const uint32_t sl = __ldg(a.hot_slot + row);
       if (sl != 0xFFu) {
-        float *h = hacc + sl * a.ldr + col;
-        atomicAdd(h, x.x);
-        atomicAdd(h + 1, x.y);
-        atomicAdd(h + 2, x.z);
-        atomicAdd(h + 3, x.w);
+        double *h = hacc + sl * a.ldr + col;
+        atomicAdd(h, (double)x.x);
+        atomicAdd(h + 1, (double)x.y);
+        atomicAdd(h + 2, (double)x.z);
+        atomicAdd(h + 3, (double)x.w);
         return;
       }
     }
-    atomicAdd(reinterpret_cast<float4 *>(a.out + (size_t)row * a.ldr + col), x);
+    double *o = a.out + (size_t)row * a.ldr + col;
+    atomicAdd(o, (double)x.x);
+    atomicAdd(o + 1, (double)x.y);
+    atomicAdd(o + 2, (double)x.z);
+    atomicAdd(o + 3, (double)x.w);
   };
   // without hot rows the grid covers every chunk: one chunk per warp
   for (uint32_t chunk_id = blockIdx.x * kWarps + warp; chunk_id < a.nchunks;
@@ -779,8 +810,8 @@ __global__ void __launch_bounds__(256, HOT ? 3 : 1) k_scatter(const __grid_const
   if constexpr (HOT) {
     __syncthreads();
     for (int i = threadIdx.x; i < a.nhot * a.ldr; i += blockDim.x) {
-      const float v = hacc[i];
-      if (v != 0.f) atomicAdd(a.out + (size_t)a.hot_rows[i / a.ldr] * a.ldr + i % a.ldr, v);
+      const double v = hacc[i];
+      if (v != 0.0) atomicAdd(a.out + (size_t)a.hot_rows[i / a.ldr] * a.ldr + i % a.ldr, v);
     }
   }
 }
@@ -824,19 +855,6 @@ __global__ void k_schedule(WalkArgs a, uint32_t *sched) {
   sched[(size_t)c * (S + 1) + S] = mask;
 }
 
-// Zero the memo rows that chunk boundaries cut (they are filled by atomics).
-__global__ void k_prezero(WalkArgs a, const uint32_t *sched) {
-  const uint32_t c = blockIdx.x * blockDim.y + threadIdx.y;
-  if (c >= a.nchunks || c == 0) return;
-  const int S = a.S;
-  const uint32_t mask = sched[(size_t)c * (S + 1) + S];
-  for (int l = a.d; l < S; ++l) {
-    if (a.store[l] == nullptr || !((mask >> l) & 1u)) continue;
-    const uint32_t n = sched[(size_t)c * (S + 1) + l];
-    for (int r = threadIdx.x; r < a.ldr; r += blockDim.x) a.store[l][(size_t)n * a.ldr + r] = 0.f;
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Deterministic accumulation: chain sums of cut nodes, prefix rows, pulls.
 // ---------------------------------------------------------------------------
@@ -850,9 +868,9 @@ struct ChainArgs {
   const uint32_t *chains;  // 6 per chain
   const uint32_t *groups;  // 3 per group
   uint32_t nchains, ngroups;
-  float *gsum;
+  double *gsum;
   float *store[kMaxModes];
-  float *out;              // level-0 output rows (output level 0), else nullptr
+  double *out;             // level-0 output rows (output level 0), else nullptr
   const uint32_t *root_ids;
 };
 
@@ -877,8 +895,8 @@ __global__ void k_chain_groups(const __grid_constant__ ChainArgs a) {
   const uint32_t *c = a.chains + 6 * (size_t)ch;
   const int ls = a.span_lev[c[0]];
   for (int col = lane; col < a.R; col += 32) {
-    float acc = 0.f;
-    for (uint32_t k = k0; k < k0 + cnt; ++k) acc += chain_partial(a, ls, c[2], c[3], k)[col];
+    double acc = 0.0;
+    for (uint32_t k = k0; k < k0 + cnt; ++k) acc += (double)chain_partial(a, ls, c[2], c[3], k)[col];
     a.gsum[(size_t)g * a.ldr + col] = acc;
   }
 }
@@ -893,11 +911,11 @@ __global__ void k_chain_finish(const __grid_constant__ ChainArgs a) {
   const int l = (int)c[0];
   const uint32_t node = c[1], g0 = c[4], ng = c[5];
   float *st = a.store[l];
-  float *ot = (l == 0 && a.out) ? a.out + (size_t)a.root_ids[node] * a.ldr : nullptr;
+  double *ot = (l == 0 && a.out) ? a.out + (size_t)a.root_ids[node] * a.ldr : nullptr;
   for (int col = lane; col < a.R; col += 32) {
-    float acc = 0.f;
+    double acc = 0.0;
     for (uint32_t g = g0; g < g0 + ng; ++g) acc += a.gsum[(size_t)g * a.ldr + col];
-    if (st) st[(size_t)node * a.ldr + col] = acc;
+    if (st) st[(size_t)node * a.ldr + col] = (float)acc;
     if (ot) ot[col] = acc;
   }
 }
@@ -935,8 +953,8 @@ struct PullArgs {
   const float *vals;      // leaf values (leaf source)
   const float *src_rows;  // node rows of level d (row source)
   const float *prefix;    // P_{d-1} rows (d >= 1)
-  float *out;
-  float *piece_sum;
+  double *out;
+  double *piece_sum;
 };
 
 // Pull scatter: one warp per segment of units sorted by output row; each
@@ -953,11 +971,15 @@ __global__ void __launch_bounds__(256) k_pull(const __grid_constant__ PullArgs a
   for (uint32_t sg = blockIdx.x * kWarps + warp; sg < a.nsegs; sg += gridDim.x * kWarps) {
     const uint32_t jb = a.segs[3 * (size_t)sg], je = a.segs[3 * (size_t)sg + 1],
                    slot = a.segs[3 * (size_t)sg + 2];
-    fv<V> acc = fv_fill<V>(0.f);
+    double acc[V];
+#pragma unroll
+    for (int i = 0; i < V; ++i) acc[i] = 0.0;
     uint32_t cur = a.prow[jb];
     auto flush = [&](uint32_t row) {
-      if (slot == 0xFFFFFFFFu) st_rows<V>(a.out, row, a.ldr, col, acc, act);
-      else st_rows<V>(a.piece_sum, slot, a.ldr, col, acc, act);
+      if (!act) return;
+      double *p = (slot == 0xFFFFFFFFu ? a.out + (size_t)row * a.ldr : a.piece_sum + (size_t)slot * a.ldr) + col;
+#pragma unroll
+      for (int i = 0; i < V; ++i) p[i] = acc[i];
     };
     for (uint32_t j0 = jb; j0 < je; j0 += kBatch) {
       const int cnt = (int)min((uint32_t)kBatch, je - j0);
@@ -988,11 +1010,12 @@ __global__ void __launch_bounds__(256) k_pull(const __grid_constant__ PullArgs a
             const uint32_t row = stage[warp][k].y;
             if (row != cur) {
               flush(cur);
-              acc = fv_fill<V>(0.f);
+#pragma unroll
+              for (int i = 0; i < V; ++i) acc[i] = 0.0;
               cur = row;
             }
 #pragma unroll
-            for (int i = 0; i < V; ++i) acc.x[i] += x[q].x[i];
+            for (int i = 0; i < V; ++i) acc[i] += (double)x[q].x[i];
           }
         }
       }
@@ -1003,21 +1026,21 @@ __global__ void __launch_bounds__(256) k_pull(const __grid_constant__ PullArgs a
 }
 
 // One warp per long row: its pieces summed in order.
-__global__ void k_piece_sum(const uint32_t *pieces, uint32_t nlong, const float *piece_sum, int R,
-                            int ldr, float *out) {
+__global__ void k_piece_sum(const uint32_t *pieces, uint32_t nlong, const double *piece_sum, int R,
+                            int ldr, double *out) {
   const uint32_t i = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (i >= nlong) return;
   const uint32_t row = pieces[3 * (size_t)i], p0 = pieces[3 * (size_t)i + 1],
                  np = pieces[3 * (size_t)i + 2];
   for (int col = lane; col < R; col += 32) {
-    float acc = 0.f;
+    double acc = 0.0;
     for (uint32_t p = p0; p < p0 + np; ++p) acc += piece_sum[(size_t)p * ldr + col];
     out[(size_t)row * ldr + col] = acc;
   }
 }
 
-WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
+WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, double *out) {
   WalkArgs a;
   const DevCsf &c = *w.csf;
   a.N = w.nmodes;
@@ -1046,7 +1069,7 @@ WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, float *out) {
   a.nhot = w.nhot;
   a.hot_slot = w.hot_slot.get();
   a.hot_rows = w.hot_rows.get();
-  a.span = w.deterministic ? w.span.get() : nullptr;
+  a.span = w.span_nlev > 0 ? w.span.get() : nullptr;
   a.span_nlev = w.span_nlev;
   for (int l = 0; l < kMaxModes; ++l) a.span_lev[l] = w.span_lev[l];
   return a;
@@ -1117,7 +1140,7 @@ template <int W, FactorType FT, bool LEAF>
 void launch_scatter_w(const WalkArgs &a, unsigned blocks, cudaStream_t s) {
   if (a.nhot > 0) {
     // each block sums the hot rows once: as few blocks as fit at once
-    const size_t smem = kWarps * scatter_warp_bytes(a.ldr) + (size_t)a.nhot * a.ldr * sizeof(float);
+    const size_t smem = kWarps * scatter_warp_bytes(a.ldr) + (size_t)a.nhot * a.ldr * sizeof(double);
     blocks = std::min(blocks, resident_blocks(k_scatter<W, FT, LEAF, true>, 256, smem));
     k_scatter<W, FT, LEAF, true><<<blocks, 256, smem, s>>>(a);
   } else {
@@ -1196,7 +1219,7 @@ void set_walk_attributes() {
   ADATM_CUDA(cudaFuncSetAttribute(k_scatter<W, FT, LEAF, true>,                   \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)(kWarps * scatter_warp_bytes(128) +        \
-                                        kHotRows * 128 * sizeof(float))));
+                                        kHotRows * 128 * sizeof(double))));
 #define ADATM_ATTR_ALL(M, X)                \
   M(X, FactorType::F32, true)               \
   M(X, FactorType::F32, false)              \
@@ -1235,13 +1258,14 @@ void to_device(DevBuf<T> &dst, const std::vector<T> &h, cudaStream_t s) {
   ADATM_CUDA(cudaStreamSynchronize(s));
 }
 
-// Slots and chains of a contraction: levels whose cut nodes would take
-// atomics (stored levels, and level 0 when it is the output), and for each
-// node a chunk boundary cuts, the run of chunks it spans.
-void det_prepare_contract(TreeWalk &w, cudaStream_t s) {
+// Slots and chains of a contraction: levels whose cut nodes would otherwise
+// take atomics (stored levels, and level 0 when it is the output), and for
+// each node a chunk boundary cuts, the run of chunks it spans. Deterministic
+// contractions below the root also store their level-d sums for the pull.
+void prepare_spans(TreeWalk &w, cudaStream_t s) {
   const DevCsf &c = *w.csf;
   const int S = w.src, d = w.out;
-  if (d > 0) {
+  if (w.deterministic && d > 0) {
     // the level-d sums are stored, then pulled into the output rows
     w.level_rows.alloc((size_t)std::max<uint64_t>(c.nfibs[d], 1) * w.ldr);
     ADATM_CUDA(cudaMemsetAsync(w.level_rows.get(), 0, w.level_rows.bytes(), s));
@@ -1397,7 +1421,7 @@ void launch_prefix(const TreeWalk &w, const LevelFactors &f, cudaStream_t s) {
 }
 
 void launch_pull(const TreeWalk &w, const LevelFactors &f, FactorType ft, const float *rows,
-                 float *out, cudaStream_t s) {
+                 double *out, cudaStream_t s) {
   if (w.nsegs == 0) return;
   if (ft == FactorType::F32) launch_prefix<FactorType::F32>(w, f, s);
   else launch_prefix<FactorType::BF16>(w, f, s);
@@ -1430,7 +1454,7 @@ void launch_pull(const TreeWalk &w, const LevelFactors &f, FactorType ft, const 
   }
 }
 
-void launch_chains(const TreeWalk &w, float *out, cudaStream_t s) {
+void launch_chains(const TreeWalk &w, double *out, cudaStream_t s) {
   if (w.nchains == 0) return;
   ChainArgs a;
   a.span = w.span.get();
@@ -1508,16 +1532,13 @@ void walk_prepare(TreeWalk &w, cudaStream_t s) {
   WalkArgs a = make_args(w, nullptr, nullptr);
   k_schedule<<<(w.nchunks + 255) / 256, 256, 0, s>>>(a, w.sched.get());
   ADATM_LAUNCH();
-  if (w.deterministic) {
-    w.pull = w.src == w.out;
-    if (w.src > w.out) det_prepare_contract(w, s);
-    if (w.pull) det_prepare_pull(w, s);
-    return;
-  }
-  if (w.src == w.out && w.nunits >= kHotMin) find_hot_rows(w, s);
+  w.pull = w.deterministic && w.src == w.out;
+  if (w.src > w.out) prepare_spans(w, s);
+  if (w.pull) det_prepare_pull(w, s);
+  if (!w.deterministic && w.src == w.out && w.nunits >= kHotMin) find_hot_rows(w, s);
 }
 
-void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float *out,
+void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, double *out,
                  cudaStream_t s) {
   if (w.nchunks == 0) return;
   if (w.deterministic && w.src == w.out) {
@@ -1525,11 +1546,6 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
     return;
   }
   const WalkArgs a = make_args(w, &f, w.deterministic && w.out > 0 ? nullptr : out);
-  if (w.has_store() && !w.deterministic) {
-    dim3 blk(32, 8);
-    k_prezero<<<(w.nchunks + 7) / 8, blk, 0, s>>>(a, w.sched.get());
-    ADATM_LAUNCH();
-  }
   const unsigned blocks = (unsigned)((w.nchunks + kWarps - 1) / kWarps);
   const bool leaf = w.src == w.nmodes - 1;
   if (w.src > w.out) {
@@ -1542,10 +1558,8 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float 
       if (leaf) launch_contract<FactorType::BF16, true>(vec, wk, a, blocks, w.resident, s);
       else launch_contract<FactorType::BF16, false>(vec, wk, a, blocks, w.resident, s);
     }
-    if (w.deterministic) {
-      launch_chains(w, out, s);
-      if (w.pull) launch_pull(w, f, ft, w.level_rows.get(), out, s);
-    }
+    launch_chains(w, out, s);
+    if (w.deterministic && w.out > 0) launch_pull(w, f, ft, w.level_rows.get(), out, s);
   } else {
     const int lanes = lanes_for_rank(w.R);
     if (ft == FactorType::F32) {
@@ -1563,10 +1577,9 @@ int walk_kernels(const TreeWalk &w) {
   int k = 0;
   if (w.src > w.out) {
     k += 1;                                            // the contraction
-    if (!w.deterministic) return k + (w.has_store() ? 1 : 0);  // + the prezero of cut memo rows
     if (w.nchains) k += 2;                             // chain groups, chain finish
   }
-  if (w.deterministic && w.pull && w.nsegs) k += w.out + 1 + (w.nlong ? 1 : 0);
+  if (w.deterministic && w.nsegs) k += w.out + 1 + (w.nlong ? 1 : 0);  // prefix levels, pull, pieces
   if (!w.deterministic && w.src == w.out) k += 1;      // the scatter
   return k;
 }
@@ -1589,7 +1602,7 @@ double walk_compulsory_bytes(const TreeWalk &w, FactorType ft, const uint64_t *d
     if (l <= w.src && l != w.out) b += bf * R * (double)dims_of_level[l];  // factors
   for (int l = 0; l < kMaxModes; ++l)
     if (w.store[l]) b += 4.0 * R * (double)c.nfibs[l];     // memo rows written
-  b += 4.0 * R * (double)out_rows;                         // output
+  b += 8.0 * R * (double)out_rows;                         // output (FP64 rows)
   return b;
 }
 

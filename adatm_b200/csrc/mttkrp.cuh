@@ -57,14 +57,15 @@ struct TreeWalk {
   int nhot = 0;
   DevBuf<uint8_t> hot_slot;
   DevBuf<uint32_t> hot_rows;
-  // Deterministic accumulation (no float atomics): every output and memo
-  // row is summed in an order fixed by the tree, so repeated runs agree bit
-  // for bit. Contractions write the partial sums of the nodes chunk
-  // boundaries cut to per-chunk rows (span) and sum them per node in chunk
-  // order (chains, in groups of kChainGroup partials); scatters, and the
-  // output of contractions below the root, pull each output row's units in
-  // the order of a stable sort by output row (segments of whole rows, long
-  // rows split into pieces summed in order).
+  // Nodes that chunk boundaries cut (contractions, every mode): their
+  // partial sums go to per-chunk rows (span) and are summed per node in
+  // chunk order and in FP64 (chains, in groups of kChainGroup partials), so
+  // a node spanning thousands of chunks (a skewed root slice) takes no long
+  // chain of FP32 atomics. Deterministic accumulation additionally pulls
+  // scatters, and the output of contractions below the root, per output row
+  // in the order of a stable sort by output row (segments of whole rows, long
+  // rows split into pieces summed in order): no float atomics anywhere, so
+  // repeated runs agree bit for bit.
   bool deterministic = false;
   int span_nlev = 0;
   int span_lev[kMaxModes] = {-1, -1, -1, -1, -1, -1, -1, -1};
@@ -72,7 +73,7 @@ struct TreeWalk {
   DevBuf<uint32_t> chains;           // per chain: level, node, first boundary chunk, last chunk,
                                      // first group, groups
   DevBuf<uint32_t> groups;           // per group: chain, first partial, partials
-  DevBuf<float> gsum;                // per group: its sum (ldr)
+  DevBuf<double> gsum;               // per group: its sum (ldr)
   uint32_t nchains = 0, ngroups = 0;
   DevBuf<float> level_rows;          // contraction below the root: level-d node sums
   // pull scatter of level `out` (deterministic scatters and contractions below the root)
@@ -81,7 +82,7 @@ struct TreeWalk {
   DevBuf<uint32_t> perm, prow, pparent;  // units sorted by output row (stable), their rows, parents
   DevBuf<uint32_t> segs;             // per segment: first, end, piece slot (~0u: whole rows)
   DevBuf<uint32_t> pieces;           // per long row: row, first piece slot, pieces
-  DevBuf<float> piece_sum;           // per piece: its sum (ldr)
+  DevBuf<double> piece_sum;          // per piece: its sum (ldr)
   uint32_t nsegs = 0, nlong = 0, npieces = 0;
   DevBuf<float> prefix[2];           // prefix rows of levels 0..out-1 (ping-pong)
   bool has_store() const {
@@ -103,9 +104,9 @@ bool walkers_supported(int R, int W);
 // unit, plus a bit mask of the levels whose node began before the chunk.
 void walk_prepare(TreeWalk &w, cudaStream_t s);
 
-// Launch the walk: output rows must be zero beforehand (the caller clears
-// them); memo rows cut by chunk boundaries are zeroed here (atomic mode).
-void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, float *out,
+// Launch the walk: output rows (FP64, dims x ldr) must be zero beforehand
+// (the caller clears them).
+void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, double *out,
                  cudaStream_t s);
 
 // Bytes the walk must move through HBM (structure read once, memo rows read

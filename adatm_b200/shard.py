@@ -7,7 +7,8 @@ are replicated. A CP-ALS sweep runs mode by mode:
 
   * every rank computes its shard's MTTKRP of the mode (the memo plan works
     unchanged on the shard's own trees: an MTTKRP is linear in the nonzeros);
-  * the ranks' MTTKRPs are summed (one all-reduce of dims[mode] x ldr floats);
+  * the ranks' MTTKRPs are summed (one all-reduce of dims[mode] x ldr FP64
+    values);
   * every rank runs the same update from the sum (Gram inverse, A = M V^-1,
     normalisation, Gram, and for the last mode the fit's inner product), so
     the factors, Grams and lambda stay identical on every rank;
@@ -92,10 +93,10 @@ class ShardedCpd:
 
 
 def torch_buffers(dims, rank_count, ldr, device):
-    """One float32 device buffer per mode (dims[m] x ldr) for each of
-    rank_count local shards."""
+    """One float64 device buffer per mode (dims[m] x ldr, the MTTKRP rows'
+    FP64 sums) for each of rank_count local shards."""
     import torch
-    return [[torch.zeros(int(d) * ldr, dtype=torch.float32, device=device) for d in dims]
+    return [[torch.zeros(int(d) * ldr, dtype=torch.float64, device=device) for d in dims]
             for _ in range(rank_count)]
 
 

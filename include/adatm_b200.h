@@ -270,7 +270,7 @@ int adatm_engine_fit(adatm_engine *e, double *fit);
 /* One shard of a tensor split across ranks by root slices (each rank holds
  * an engine on its nonzeros, same dims and plan; factors are replicated).
  * A sweep runs mode by mode: adatm_engine_mttkrp_into writes this shard's
- * MTTKRP of `mode` to a device buffer (dims[mode] x ldr floats, ldr = R
+ * MTTKRP of `mode` to a device buffer (dims[mode] x ldr doubles, ldr = R
  * rounded up to 4); the caller sums the ranks' buffers (an all-reduce);
  * adatm_engine_update_from runs the mode's update from the summed buffer;
  * after the last mode adatm_engine_fit_step gives the fit. ||X||^2 is the
@@ -278,8 +278,8 @@ int adatm_engine_fit(adatm_engine *e, double *fit);
  * adatm_engine_set_ttnorm. Calls return when their work is done. Start with
  * adatm_engine_als_begin(e, 0). The reference's only collective is the fit's
  * MPI all-reduce (adatm_cpd.c:147-157); this split adds the MTTKRP sum. */
-int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, float *dev_out);
-int adatm_engine_update_from(adatm_engine *e, uint64_t mode, const float *dev_M);
+int adatm_engine_mttkrp_into(adatm_engine *e, uint64_t mode, double *dev_out);
+int adatm_engine_update_from(adatm_engine *e, uint64_t mode, const double *dev_M);
 int adatm_engine_fit_step(adatm_engine *e, double *fit);
 int adatm_engine_ttnorm(adatm_engine *e, double *local);
 int adatm_engine_set_ttnorm(adatm_engine *e, double global);
