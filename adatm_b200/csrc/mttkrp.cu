@@ -859,7 +859,7 @@ __global__ void k_schedule(WalkArgs a, uint32_t *sched) {
 // Deterministic accumulation: chain sums of cut nodes, prefix rows, pulls.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kChainGroup = 32;  // partials one warp sums per group
-constexpr uint32_t kPullSeg = 256;    // units per pull segment (whole rows) and per piece
+constexpr uint32_t kPullSeg = 256;    // units per pull segment (whole rows) and per piece, at most
 
 struct ChainArgs {
   const float *span;
@@ -895,29 +895,87 @@ __global__ void k_chain_groups(const __grid_constant__ ChainArgs a) {
   const uint32_t *c = a.chains + 6 * (size_t)ch;
   const int ls = a.span_lev[c[0]];
   for (int col = lane; col < a.R; col += 32) {
+    // loads issued eight at a time, added in chunk order
     double acc = 0.0;
-    for (uint32_t k = k0; k < k0 + cnt; ++k) acc += (double)chain_partial(a, ls, c[2], c[3], k)[col];
+    uint32_t k = k0;
+    for (; k + 8 <= k0 + cnt; k += 8) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = chain_partial(a, ls, c[2], c[3], k + q)[col];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc += (double)v[q];
+    }
+    for (; k < k0 + cnt; ++k) acc += (double)chain_partial(a, ls, c[2], c[3], k)[col];
     a.gsum[(size_t)g * a.ldr + col] = acc;
   }
 }
 
-// One warp per chain: the group sums in order, stored to the node's memo row
-// and, at level 0 with a root output, to its output row.
-__global__ void k_chain_finish(const __grid_constant__ ChainArgs a) {
-  const uint32_t ch = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (ch >= a.nchains) return;
-  const uint32_t *c = a.chains + 6 * (size_t)ch;
-  const int l = (int)c[0];
-  const uint32_t node = c[1], g0 = c[4], ng = c[5];
-  float *st = a.store[l];
-  double *ot = (l == 0 && a.out) ? a.out + (size_t)a.root_ids[node] * a.ldr : nullptr;
-  for (int col = lane; col < a.R; col += 32) {
-    double acc = 0.0;
-    for (uint32_t g = g0; g < g0 + ng; ++g) acc += a.gsum[(size_t)g * a.ldr + col];
-    if (st) st[(size_t)node * a.ldr + col] = (float)acc;
-    if (ot) ot[col] = acc;
+// Sum of n FP64 rows (stride ldr) in index order, column col: loads issued
+// eight at a time.
+__device__ __forceinline__ double ordered_sum(const double *rows, uint64_t n, int ldr, int col) {
+  double acc = 0.0;
+  uint64_t k = 0;
+  for (; k + 8 <= n; k += 8) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = rows[(k + q) * ldr + col];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc += v[q];
   }
+  for (; k < n; ++k) acc += rows[k * ldr + col];
+  return acc;
+}
+
+// Sum of n FP64 rows in index order by a whole block: warp w sums the w-th
+// of 8 contiguous ranges, then the 8 range sums are added in order. The
+// split depends only on n, so the result does not depend on scheduling.
+__device__ __forceinline__ void block_ordered_sum(const double *rows, uint64_t n, int ldr, int R,
+                                                  double *red /* kWarps x R */, double *out_col) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t per = (n + kWarps - 1) / kWarps;
+  const uint64_t b = min(n, (uint64_t)warp * per), e = min(n, b + per);
+  for (int col = lane; col < R; col += 32)
+    red[warp * R + col] = ordered_sum(rows + b * ldr, e - b, ldr, col);
+  __syncthreads();
+  if (warp == 0)
+    for (int col = lane; col < R; col += 32) {
+      double acc = 0.0;
+      for (int w = 0; w < kWarps; ++w) acc += red[w * R + col];
+      out_col[col] = acc;
+    }
+  __syncthreads();
+}
+
+// A chain's total, stored to the node's memo row and, at level 0 with a
+// root output, to its output row.
+__device__ __forceinline__ void chain_store(const ChainArgs &a, const uint32_t *c, int col, double v) {
+  const int l = (int)c[0];
+  const uint32_t node = c[1];
+  if (a.store[l]) a.store[l][(size_t)node * a.ldr + col] = (float)v;
+  if (l == 0 && a.out) a.out[(size_t)a.root_ids[node] * a.ldr + col] = v;
+}
+
+// Chains of at most kChainShort groups: one warp each, the group sums in
+// order.
+constexpr uint32_t kChainShort = 16;
+__global__ void k_chain_finish(const __grid_constant__ ChainArgs a, const uint32_t *ids, uint32_t n) {
+  const uint32_t i = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const uint32_t *c = a.chains + 6 * (size_t)ids[i];
+  for (int col = lane; col < a.R; col += 32)
+    chain_store(a, c, col, ordered_sum(a.gsum + (size_t)c[4] * a.ldr, c[5], a.ldr, col));
+}
+
+// Longer chains (a skewed root slice cut by thousands of chunks): one block
+// each.
+__global__ void __launch_bounds__(256) k_chain_finish_long(const __grid_constant__ ChainArgs a,
+                                                           const uint32_t *ids) {
+  __shared__ double red[kWarps * 128];
+  __shared__ double tot[128];
+  const uint32_t *c = a.chains + 6 * (size_t)ids[blockIdx.x];
+  block_ordered_sum(a.gsum + (size_t)c[4] * a.ldr, c[5], a.ldr, a.R, red, tot);
+  for (int col = threadIdx.x; col < a.R; col += blockDim.x) chain_store(a, c, col, tot[col]);
 }
 
 // parent[c] = p for the children c of every node p (fptr of the parent level).
@@ -1025,19 +1083,16 @@ __global__ void __launch_bounds__(256) k_pull(const __grid_constant__ PullArgs a
   }
 }
 
-// One warp per long row: its pieces summed in order.
-__global__ void k_piece_sum(const uint32_t *pieces, uint32_t nlong, const double *piece_sum, int R,
-                            int ldr, double *out) {
-  const uint32_t i = (uint32_t)((blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (i >= nlong) return;
+// One block per long row: its pieces summed in order.
+__global__ void __launch_bounds__(256) k_piece_sum(const uint32_t *pieces, const double *piece_sum,
+                                                   int R, int ldr, double *out) {
+  __shared__ double red[kWarps * 128];
+  __shared__ double tot[128];
+  const uint32_t i = blockIdx.x;
   const uint32_t row = pieces[3 * (size_t)i], p0 = pieces[3 * (size_t)i + 1],
                  np = pieces[3 * (size_t)i + 2];
-  for (int col = lane; col < R; col += 32) {
-    double acc = 0.0;
-    for (uint32_t p = p0; p < p0 + np; ++p) acc += piece_sum[(size_t)p * ldr + col];
-    out[(size_t)row * ldr + col] = acc;
-  }
+  block_ordered_sum(piece_sum + (size_t)p0 * ldr, np, ldr, R, red, tot);
+  for (int col = threadIdx.x; col < R; col += blockDim.x) out[(size_t)row * ldr + col] = tot[col];
 }
 
 WalkArgs make_args(const TreeWalk &w, const LevelFactors *f, double *out) {
@@ -1311,6 +1366,14 @@ void prepare_spans(TreeWalk &w, cudaStream_t s) {
   }
   w.nchains = (uint32_t)(chains.size() / 6);
   w.ngroups = (uint32_t)(groups.size() / 3);
+  // short chains first (a warp each), then long ones (a block each)
+  std::vector<uint32_t> ids;
+  for (uint32_t i = 0; i < w.nchains; ++i)
+    if (chains[6 * (size_t)i + 5] <= kChainShort) ids.push_back(i);
+  w.nshort = (uint32_t)ids.size();
+  for (uint32_t i = 0; i < w.nchains; ++i)
+    if (chains[6 * (size_t)i + 5] > kChainShort) ids.push_back(i);
+  to_device(w.chain_ids, ids, s);
   to_device(w.chains, chains, s);
   to_device(w.groups, groups, s);
   w.gsum.alloc((size_t)std::max<uint32_t>(w.ngroups, 1) * w.ldr);
@@ -1346,7 +1409,10 @@ void det_prepare_pull(TreeWalk &w, cudaStream_t s) {
       if (d >= 1) pparent[j] = par[u];
     }
   }
-  // segments: whole rows packed up to kPullSeg units; longer rows in pieces
+  // segments: whole rows packed up to `seg` units (kPullSeg, shorter for
+  // small levels so the segments still fill the device); longer rows in pieces
+  uint64_t seg = kPullSeg;
+  while (seg > 32 && n / seg < 148ull * 32) seg /= 2;
   std::vector<uint32_t> segs, pieces;
   uint32_t npieces = 0;
   uint64_t seg_start = 0, seg_len = 0;
@@ -1362,22 +1428,22 @@ void det_prepare_pull(TreeWalk &w, cudaStream_t s) {
   for (uint64_t r = 0; r < rows; ++r) {
     const uint64_t b = start[r], cnt = start[r + 1] - b;
     if (cnt == 0) continue;
-    if (cnt > kPullSeg) {
+    if (cnt > seg) {
       close_seg(b);
-      const uint32_t np = (uint32_t)((cnt + kPullSeg - 1) / kPullSeg);
+      const uint32_t np = (uint32_t)((cnt + seg - 1) / seg);
       pieces.push_back((uint32_t)r);
       pieces.push_back(npieces);
       pieces.push_back(np);
       for (uint32_t q = 0; q < np; ++q) {
-        segs.push_back((uint32_t)(b + (uint64_t)q * kPullSeg));
-        segs.push_back((uint32_t)std::min<uint64_t>(b + (uint64_t)(q + 1) * kPullSeg, b + cnt));
+        segs.push_back((uint32_t)(b + (uint64_t)q * seg));
+        segs.push_back((uint32_t)std::min<uint64_t>(b + (uint64_t)(q + 1) * seg, b + cnt));
         segs.push_back(npieces + q);
       }
       npieces += np;
       seg_start = b + cnt;
       continue;
     }
-    if (seg_len + cnt > kPullSeg) close_seg(b);
+    if (seg_len + cnt > seg) close_seg(b);
     seg_len += cnt;
   }
   close_seg(n);
@@ -1448,8 +1514,7 @@ void launch_pull(const TreeWalk &w, const LevelFactors &f, FactorType ft, const 
   }
   ADATM_LAUNCH();
   if (w.nlong) {
-    k_piece_sum<<<(w.nlong * 32 + 255) / 256, 256, 0, s>>>(w.pieces.get(), w.nlong, w.piece_sum.get(),
-                                                             w.R, w.ldr, out);
+    k_piece_sum<<<w.nlong, 256, 0, s>>>(w.pieces.get(), w.piece_sum.get(), w.R, w.ldr, out);
     ADATM_LAUNCH();
   }
 }
@@ -1474,8 +1539,15 @@ void launch_chains(const TreeWalk &w, double *out, cudaStream_t s) {
   a.root_ids = w.csf->fids[0].get();
   k_chain_groups<<<(unsigned)(((uint64_t)w.ngroups * 32 + 255) / 256), 256, 0, s>>>(a);
   ADATM_LAUNCH();
-  k_chain_finish<<<(unsigned)(((uint64_t)w.nchains * 32 + 255) / 256), 256, 0, s>>>(a);
-  ADATM_LAUNCH();
+  if (w.nshort) {
+    k_chain_finish<<<(unsigned)(((uint64_t)w.nshort * 32 + 255) / 256), 256, 0, s>>>(
+        a, w.chain_ids.get(), w.nshort);
+    ADATM_LAUNCH();
+  }
+  if (w.nchains > w.nshort) {
+    k_chain_finish_long<<<w.nchains - w.nshort, 256, 0, s>>>(a, w.chain_ids.get() + w.nshort);
+    ADATM_LAUNCH();
+  }
 }
 
 }  // namespace
@@ -1577,7 +1649,7 @@ int walk_kernels(const TreeWalk &w) {
   int k = 0;
   if (w.src > w.out) {
     k += 1;                                            // the contraction
-    if (w.nchains) k += 2;                             // chain groups, chain finish
+    if (w.nchains) k += 1 + (w.nshort ? 1 : 0) + (w.nchains > w.nshort ? 1 : 0);  // chain sums
   }
   if (w.deterministic && w.nsegs) k += w.out + 1 + (w.nlong ? 1 : 0);  // prefix levels, pull, pieces
   if (!w.deterministic && w.src == w.out) k += 1;      // the scatter

@@ -75,6 +75,8 @@ struct TreeWalk {
   DevBuf<uint32_t> groups;           // per group: chain, first partial, partials
   DevBuf<double> gsum;               // per group: its sum (ldr)
   uint32_t nchains = 0, ngroups = 0;
+  DevBuf<uint32_t> chain_ids;        // chains of few groups first (nshort), then long ones
+  uint32_t nshort = 0;
   DevBuf<float> level_rows;          // contraction below the root: level-d node sums
   // pull scatter of level `out` (deterministic scatters and contractions below the root)
   bool pull = false;
