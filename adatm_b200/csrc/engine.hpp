@@ -24,9 +24,11 @@ struct EngineOptions {
   bool resident_grid = true;
   // walkers per warp in the contraction source loop (0 = default_walkers(R))
   int walkers = 0;
-  // no float atomics: every MTTKRP output and memo row is summed in an
-  // order fixed by the tree, so sweeps repeat bit for bit
-  bool deterministic = false;
+  // no float atomics (the default): every MTTKRP output and memo row is
+  // summed in an order fixed by the tree, in FP64 across chunks, so sweeps
+  // repeat bit for bit; off, scatters add into the FP64 output rows with
+  // atomics
+  bool deterministic = true;
 };
 
 class Engine {

@@ -316,15 +316,18 @@ int adatm_engine_set_resident_grid(adatm_engine *e, int on);
  * counterpart (a launch-shape control). */
 int adatm_engine_set_walkers(adatm_engine *e, int walkers);
 
-/* Deterministic accumulation (on != 0): no float atomics anywhere in the
- * MTTKRPs. Contractions write the partial sums of the tree nodes that chunk
- * boundaries cut to per-chunk rows and sum them per node in chunk order;
- * scatters (and contractions whose output level is below the root) visit
- * every output row's contributions in a stable order by row. Sweeps then
- * repeat bit for bit from the same start, on one device and build. Costs
- * extra device memory (per-chunk rows, sorted unit lists, prefix rows) and
- * time. Drops a captured sweep. No reference counterpart: the reference's
- * locked OpenMP scatters (mttkrp.c:13-14,121-125) sum in thread order. */
+/* Deterministic accumulation, on by default (on != 0): no float atomics
+ * anywhere in the MTTKRPs. Contractions write the partial sums of the tree
+ * nodes that chunk boundaries cut to per-chunk rows and sum them per node in
+ * chunk order (always, in both settings); scatters, and contractions whose
+ * output level is below the root, visit every output row's contributions in
+ * a stable order by row. Output rows are FP64 sums. Sweeps then repeat bit
+ * for bit from the same start, on one device and build. Costs extra device
+ * memory (per-chunk rows, sorted unit lists, prefix rows). Off (on == 0),
+ * scatters add into the FP64 output rows with atomics (order-dependent in
+ * the last bits). Drops a captured sweep. No reference counterpart: the
+ * reference's locked OpenMP scatters (mttkrp.c:13-14,121-125) sum in thread
+ * order. */
 int adatm_engine_set_deterministic(adatm_engine *e, int on);
 
 /* One ALS iteration of every engine in one CUDA graph (each engine on its
