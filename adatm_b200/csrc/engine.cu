@@ -182,7 +182,7 @@ void Engine::set_walkers(int walkers) {
   opt_.walkers = walkers;
   for (int m = 0; m < coo_->nmodes; ++m) {
     walk_[m]->walkers = walkers;
-    direct_[m]->walkers = walkers;
+    if (direct_[m]) direct_[m]->walkers = walkers;
   }
   for (auto &kv : custom_) kv.second->walkers = walkers;
 }
@@ -192,7 +192,7 @@ void Engine::set_resident_grid(bool on) {
   opt_.resident_grid = on;
   for (int m = 0; m < coo_->nmodes; ++m) {
     walk_[m]->resident = on;
-    direct_[m]->resident = on;
+    if (direct_[m]) direct_[m]->resident = on;
   }
   for (auto &kv : custom_) kv.second->resident = on;
 }
@@ -405,7 +405,7 @@ void Engine::build_walks() {
   for (int m = 0; m < coo_->nmodes; ++m) {
     const int g = (int)plan_.use_csfs[m];
     walk_[m] = make_walk(m, g, (int)plan_.use_tags[m]);
-    direct_[m] = make_walk(m, g, 2);
+    direct_[m].reset();  // built on first use (mttkrp_direct)
   }
 }
 
@@ -476,6 +476,7 @@ FactorType Engine::sweep_type(int mode) const {
 
 void Engine::mttkrp_direct(int mode, double *out) {
   ADATM_CUDA(cudaMemsetAsync(out, 0, (size_t)coo_->dims[mode] * ldr_ * sizeof(double), stream_));
+  if (!direct_[mode]) direct_[mode] = make_walk(mode, (int)plan_.use_csfs[mode], 2);
   walk_launch(*direct_[mode], level_factors((int)plan_.use_csfs[mode], opt_.factor_type),
               opt_.factor_type, out, stream_);
 }
