@@ -84,3 +84,24 @@ def test_resident_and_per_warp_grids_agree(gpu, R):
             assert np.max(np.abs(a - b)) <= 2e-5 * max(1e-30, np.max(np.abs(a))), (k, m)
         e0.free()
         e1.free()
+
+
+@pytest.mark.slow
+def test_batch_of_64_repeats_and_tracks_fp64():
+    """The 64-tensor batch (orders 3-5, dims 100..50000, 1e4..2e6 draws,
+    uniform or Zipf indices, R = 16): two batched runs of 20 iterations from
+    the same start agree bit for bit, and every tensor's fit is within 1e-4
+    of the FP64 run of the reference's ALS steps."""
+    import subprocess
+    import sys
+    import json
+    import os
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-m", "adatm_b200.batch_case", "--tensors", "64",
+                          "--sweeps", "18", "--no-tune", "--fp64-check"], cwd=root,
+                         capture_output=True, text=True, timeout=1800)
+    assert out.returncode == 0, out.stderr[-2000:]
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    assert res["batched_reruns_identical"]
+    assert res["max_fit_difference_sequential_rerun"] == 0.0
+    assert res["fp64_fit_distance"]["max"] < 1e-4, res["fp64_fit_distance"]
