@@ -51,11 +51,12 @@ def main():
     print(f"nnz {t.info()[1]} plan {plan['groups']} fit {res['fit']:.6f} trace {res['trace']}")
     if a.time:
         n = len(dims)
+        tags = plan.get("use_tags") or A.decide_use_csfs(n, plan["groups"])[1]
         for m in range(n):
             e.time_mttkrp(m, 3)
             ms = e.time_mttkrp(m, 20) / 20
             gbs = e.mttkrp_bytes(m) / (ms * 1e-3) / 1e9
-            print(f"mode {m} tag {plan['use_tags'][m]}: {ms * 1e3:8.1f} us  {gbs:7.1f} GB/s compulsory")
+            print(f"mode {m} tag {tags[m]}: {ms * 1e3:8.1f} us  {gbs:7.1f} GB/s compulsory")
         e.als_begin(graph=True)
         e.time_sweeps(3)
         print(f"sweep (graph): {e.time_sweeps(50) / 50:.3f} ms")

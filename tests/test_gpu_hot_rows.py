@@ -1,6 +1,6 @@
-"""Scatter walks whose output rows are hit by very many units sum those rows
-per block in shared memory; the MTTKRP must not change (FP32 summation order
-aside). Tensors are built so that one output row takes about half of the
+"""Atomic scatter walks (deterministic accumulation off) whose output rows
+are hit by very many units sum those rows per block in shared memory; the
+MTTKRP must not change (FP32 summation order aside). Tensors are built so that one output row takes about half of the
 units of a leaf scatter and of a memo-reuse scatter (the hot mode has a
 large dimension, so plans place it below the root, where it is scattered).
 """
@@ -42,6 +42,7 @@ def test_hot_output_rows(gpu, R, case):
     hot_walks = 0
     for plan in plans:
         e = A.Engine(t, R, plan)
+        e.set_deterministic(False)
         e.set_factors(mats)
         om = O.Model(ci, cv, cd, R, plan["groups"]) if "use_csfs" not in plan else None
         for m in range(len(cd)):
