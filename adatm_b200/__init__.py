@@ -791,6 +791,11 @@ class Engine:
         the default for the rank)."""
         _check(lib().adatm_engine_set_walkers(self._h, int(walkers)), "adatm_engine_set_walkers")
 
+    def set_fold(self, fold):
+        """Unstored levels folded into the contraction source loop (0, 1, 2;
+        -1 = chosen from each tree's fan-out)."""
+        _check(lib().adatm_engine_set_fold(self._h, int(fold)), "adatm_engine_set_fold")
+
     def set_deterministic(self, on=True):
         """Deterministic accumulation (no float atomics): sweeps repeat bit
         for bit from the same start."""

@@ -158,6 +158,7 @@ _SIGS = [
                                         C.c_int, C.c_int, C.POINTER(C.c_int)]),
     ("adatm_engine_set_resident_grid", C.c_int, [C.c_void_p, C.c_int]),
     ("adatm_engine_set_walkers", C.c_int, [C.c_void_p, C.c_int]),
+    ("adatm_engine_set_fold", C.c_int, [C.c_void_p, C.c_int]),
     ("adatm_engine_set_deterministic", C.c_int, [C.c_void_p, C.c_int]),
     ("adatm_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)]),
     ("adatm_batch_begin", C.c_int, [C.c_void_p]),

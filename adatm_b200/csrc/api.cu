@@ -1327,6 +1327,14 @@ int adatm_engine_set_walkers(adatm_engine *e, int walkers) {
   });
 }
 
+int adatm_engine_set_fold(adatm_engine *e, int fold) {
+  return guarded([&] {
+    if (!e) throw BadInput("adatm_engine_set_fold: null engine");
+    e->eng->set_fold(fold);
+    e->graph = false;
+  });
+}
+
 int adatm_engine_set_deterministic(adatm_engine *e, int on) {
   return guarded([&] {
     if (!e) throw BadInput("adatm_engine_set_deterministic: null engine");

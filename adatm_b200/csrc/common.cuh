@@ -47,9 +47,10 @@ inline void check_cuda(cudaError_t e, const char *what, const char *file, int li
 
 inline int ldr_of(uint64_t R) { return (int)((R + 3) / 4 * 4); }
 
+// (not volatile: a pure function of the lane, so the compiler may reuse it)
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
-  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
 }
 

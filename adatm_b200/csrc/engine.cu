@@ -187,6 +187,17 @@ void Engine::set_walkers(int walkers) {
   for (auto &kv : custom_) kv.second->walkers = walkers;
 }
 
+void Engine::set_fold(int fold) {
+  if (fold < -1 || fold > 2) throw BadInput("folded levels must be -1 (automatic), 0, 1 or 2");
+  drop_graph();
+  opt_.fold = fold;
+  for (int m = 0; m < coo_->nmodes; ++m) {
+    walk_[m]->fold = fold;
+    if (direct_[m]) direct_[m]->fold = fold;
+  }
+  for (auto &kv : custom_) kv.second->fold = fold;
+}
+
 void Engine::set_resident_grid(bool on) {
   drop_graph();
   opt_.resident_grid = on;
@@ -383,6 +394,7 @@ std::unique_ptr<TreeWalk> Engine::make_walk(int mode, int g, int tag) {
   w->chunk = opt_.chunk_leaf;
   w->resident = opt_.resident_grid;
   w->walkers = opt_.walkers;
+  w->fold = opt_.fold;
   w->deterministic = opt_.deterministic;
   if (tag == 0 && gp.n_imten > 0) {
     // memo root: store level begin_imten-1-deg into memo tree deg

@@ -24,6 +24,9 @@ struct EngineOptions {
   bool resident_grid = true;
   // walkers per warp in the contraction source loop (0 = default_walkers(R))
   int walkers = 0;
+  // unstored levels folded into the contraction source loop (0..2; -1 =
+  // chosen from each tree's fan-out)
+  int fold = -1;
   // no float atomics (the default): every MTTKRP output and memo row is
   // summed in an order fixed by the tree, in FP64 across chunks, so sweeps
   // repeat bit for bit; off, scatters add into the FP64 output rows with
@@ -137,6 +140,9 @@ class Engine {
   // Walkers per warp of the contraction walks (1, 2, 4; 0 = the default
   // for the rank); drops a captured sweep.
   void set_walkers(int walkers);
+  // Levels folded into the contraction source loop (0, 1, 2; -1 = chosen
+  // from the fan-out); drops a captured sweep.
+  void set_fold(int fold);
   // Deterministic accumulation on or off (rebuilds the walks, drops a
   // captured sweep; factors, Grams and memo rows stay).
   void set_deterministic(bool on);

@@ -340,11 +340,18 @@ constexpr int contract_min_blocks() {
 }
 
 //
-// FUSE (level S-1 is not stored and lies below d): the nodes of level S-1
-// are not formed. Each unit's product is multiplied by its parent's factor
-// row (U_{S-1} of the level-(S-1) node holding it) and summed straight into
-// the open node of level S-2, so the batch's items are level-(S-2) nodes.
-// The sums equal the unfused ones up to FP32 rounding order.
+// FOLD F (levels S-1 .. S-F are not stored and lie below d): the nodes of
+// those levels are not formed. Each unit's product is multiplied by the
+// factor rows of its ancestors at levels S-1 .. S-F (U_{S-1} of the
+// level-(S-1) node holding it, and at F = 2 U_{S-2} of the level-(S-2) node
+// holding that) and summed straight into the open node of level S-1-F, so
+// the batch's items are level-(S-1-F) nodes. The ancestors of a batch's
+// units are consecutive nodes from each level's open node on (a unit's is
+// the open node plus the closes of that level before it), so their ids come
+// with one coalesced load per level. Folding trades one item of level l for
+// one extra gather per unit below it: it pays where levels are hypersparse
+// (few units per node). The sums equal the unfolded ones up to FP32
+// rounding order.
 // WALKERS: the source loop of a batch runs as W walkers of 32/W lanes, each
 // over its own contiguous segment of 32/W units with VW columns per lane, so
 // one warp instruction advances W units. Each walker sums its segment into
@@ -355,9 +362,10 @@ constexpr int contract_min_blocks() {
 // level loop keeps the warp-wide layout (V columns per lane); items and
 // carry rows are plain column-ordered rows in shared memory, so both
 // layouts read them.
-template <int V, int W, int VW, FactorType FT, bool LEAF, bool FUSE>
+template <int V, int W, int VW, FactorType FT, bool LEAF, int F>
 __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     k_contract(const __grid_constant__ WalkArgs a) {
+  static_assert(F >= 0 && F <= 2, "folded levels");
   static_assert(W == 1 || W == 2 || W == 4, "walkers per warp");
   static_assert((32 / W) * VW <= 32 * V, "a walker's columns must fit the item rows");
   constexpr int L = 32 / W;        // lanes per walker
@@ -391,13 +399,14 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     for (int l = d; l < S - 1; ++l) carry[l * 32 + lane] = fv_fill<V>(0.f);
     if (d > 0) refresh_prefix<V, FT>(a, pre, nodeL, 0, d, col, act, lane);
     const RowSrc<VW, FT> Us(a.U_src, a.ldr, wcol, wact);
-    const RowSrc<VW, FT> Up(FUSE ? a.U[S - 1] : a.U_src, a.ldr, wcol, wact);
-    const int top = FUSE ? S - 2 : S - 1;  // level whose open node the units feed
+    const RowSrc<VW, FT> Up(F >= 1 ? a.U[S - 1] : a.U_src, a.ldr, wcol, wact);
+    const RowSrc<VW, FT> Uq(F >= 2 ? a.U[S - 2] : a.U_src, a.ldr, wcol, wact);
+    const int top = S - 1 - F;  // level whose open node the units feed
     // open node of level `top` carried in from earlier batches (every walker
     // holds the same copy)
     fv<VW> acc = fv_fill<VW>(0.f);
     // unit rows in flight per lane, never more than the walker's segment
-    constexpr int SB = ((FUSE ? 8 : 16) / VW) < SEG ? ((FUSE ? 8 : 16) / VW) : SEG;
+    constexpr int SB = ((F ? 8 : 16) / VW) < SEG ? ((F ? 8 : 16) / VW) : SEG;
     static_assert(SEG % SB == 0, "a walker's segment is a whole number of load groups");
     const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
     const uint64_t u1 = min(u0 + a.chunk, a.nunits);
@@ -409,14 +418,21 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       if constexpr (LEAF) v = in ? __ldg(a.vals + base + lane) : 0.f;
       const uint32_t cd = in ? (uint32_t)__ldg(a.src_cd + base + lane) : 0u;
       const uint32_t M = __ballot_sync(~0u, cd >= 1u);
-      uint32_t pfid = 0u;
-      if constexpr (FUSE) {
+      uint32_t pfid = 0u, qfid = 0u, M2 = 0u;
+      if constexpr (F >= 1) {
         // unit lane sits in level-(S-1) node first + (closes before it)
         const uint64_t pn = (uint64_t)__shfl_sync(~0u, nodeL, S - 1) + __popc(M & lanemask_lt());
         if (in && pn < a.nfibs[S - 1]) pfid = __ldg(a.fids[S - 1] + pn);
       }
-      const uint32_t Mc = FUSE ? __ballot_sync(~0u, cd >= 2u) : M;  // closes of level `top`
-      ustage[ustage_slot(lane)] = make_uint4(id, __float_as_uint(v), pfid, 0u);
+      if constexpr (F >= 2) {
+        // and in level-(S-2) node first + (level-(S-2) closes before it)
+        M2 = __ballot_sync(~0u, cd >= 2u);
+        const uint64_t qn = (uint64_t)__shfl_sync(~0u, nodeL, S - 2) + __popc(M2 & lanemask_lt());
+        if (in && qn < a.nfibs[S - 2]) qfid = __ldg(a.fids[S - 2] + qn);
+      }
+      // closes of level `top`
+      const uint32_t Mc = F == 0 ? M : (F == 1 ? __ballot_sync(~0u, cd >= 2u) : __ballot_sync(~0u, cd >= 3u));
+      ustage[ustage_slot(lane)] = make_uint4(id, __float_as_uint(v), pfid, qfid);
       __syncwarp();
       // this walker's units are k_lo .. k_lo + SEG - 1: its closes, and the
       // item index of its first close
@@ -436,7 +452,8 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
         for (int q0 = 0; q0 < SEG; q0 += SB) {
           if (!FULL && k_lo + q0 >= cnt) break;
           fv<VW> g[SB];
-          fv<VW> h[FUSE ? SB : 1];
+          fv<VW> h[F >= 1 ? SB : 1];
+          fv<VW> h2[F >= 2 ? SB : 1];
           fv<VW> m[LEAF ? 1 : SB];
           float vv[LEAF ? SB : 1];
 #pragma unroll
@@ -447,7 +464,8 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
             const bool ok = FULL || k < cnt;
             const uint4 e = ustage[ustage_slot(k)];
             g[q] = Us.load(e.x, ok);
-            if constexpr (FUSE) h[q] = Up.load(e.z, ok);
+            if constexpr (F >= 1) h[q] = Up.load(e.z, ok);
+            if constexpr (F >= 2) h2[q] = Uq.load(e.w, ok);
             if constexpr (LEAF) vv[q] = __uint_as_float(e.y);
             if constexpr (!LEAF) m[q] = ld_rows<VW>(a.src_rows, base + k, a.ldr, wcol, ok && wact);
           }
@@ -455,9 +473,14 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
           for (int q = 0; q < SB; ++q) {
             const int k = k_lo + q0 + q;
             if (FULL || k < cnt) {
-              if constexpr (FUSE) {
-                const fv<VW> x = LEAF ? fv_scale(vv[LEAF ? q : 0], g[q]) : fv_mul(m[LEAF ? 0 : q], g[q]);
-                fv_fma(wacc, x, h[FUSE ? q : 0]);
+              if constexpr (F >= 1) {
+                fv<VW> x = LEAF ? fv_scale(vv[LEAF ? q : 0], g[q]) : fv_mul(m[LEAF ? 0 : q], g[q]);
+                if constexpr (F >= 2) {
+                  x = fv_mul(x, h[q]);
+                  fv_fma(wacc, x, h2[F >= 2 ? q : 0]);
+                } else {
+                  fv_fma(wacc, x, h[F >= 1 ? q : 0]);
+                }
               } else if constexpr (LEAF) {
                 fv_axpy(wacc, vv[LEAF ? q : 0], g[q]);
               } else {
@@ -506,12 +529,16 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
       __syncwarp();
       if ((Mc >> (cnt - 1)) & 1u) touched &= ~(1u << top);
       else touched |= 1u << top;
-      if (FUSE && M != 0u) {
+      if (F >= 1 && M != 0u) {
         if (lane == S - 1) nodeL += (uint32_t)__popc(M);
         part &= ~(1u << (S - 1));
       }
+      if (F >= 2 && M2 != 0u) {
+        if (lane == S - 2) nodeL += (uint32_t)__popc(M2);
+        part &= ~(1u << (S - 2));
+      }
       int n = __popc(Mc);
-      uint32_t icd = compact_bits(Mc, cd - (FUSE ? 2u : 1u), xbuf, lane);
+      uint32_t icd = compact_bits(Mc, cd - (uint32_t)(F + 1), xbuf, lane);
       // the level loop: items of level l (node sums that closed in this batch)
       for (int l = top; l >= d && n > 0; --l) {
         const uint32_t first = __shfl_sync(~0u, nodeL, l);
@@ -1140,10 +1167,10 @@ unsigned resident_blocks(K kernel, int threads, size_t smem) {
   return (unsigned)std::max(1, sms * std::max(1, per_sm));
 }
 
-template <int V, int W, int VW, FactorType FT, bool LEAF, bool FUSE>
+template <int V, int W, int VW, FactorType FT, bool LEAF, int F>
 void launch_contract_v(const WalkArgs &a, unsigned blocks, bool resident, cudaStream_t s) {
   const size_t smem = contract_smem<V>(a.N);
-  auto kern = k_contract<V, W, VW, FT, LEAF, FUSE>;
+  auto kern = k_contract<V, W, VW, FT, LEAF, F>;
   if (resident) {
     blocks = std::min(blocks, resident_blocks(kern, 256, smem));
     ADATM_CUDA(cudaMemsetAsync(a.counter, 0, sizeof(uint32_t), s));
@@ -1155,9 +1182,20 @@ void launch_contract_v(const WalkArgs &a, unsigned blocks, bool resident, cudaSt
   }
 }
 
-// Level S-1 can be folded into the source loop when it is neither stored nor
-// the output level.
-bool fusable(const WalkArgs &a) { return a.S - 1 > a.d && a.store[a.S - 1] == nullptr; }
+// Levels folded into the source loop: level S-1 whenever it is neither
+// stored nor the output level (a level-(S-1) item costs more than the extra
+// gather per unit at any fan-out the trees show); level S-2 as well when it
+// too is unstored and above d and holds at most kFold2Units source units per
+// node on average (at higher fan-out the extra gather per unit costs more
+// than the items it saves). `want` >= 0 caps the count.
+constexpr double kFold2Units = 4.0;
+int fold_levels(const WalkArgs &a, int want) {
+  const int cap = want < 0 ? 2 : std::min(want, 2);
+  int f = 0;
+  while (f < cap && a.S - 1 - f > a.d && a.store[a.S - 1 - f] == nullptr) ++f;
+  if (want < 0 && f == 2 && (double)a.nunits > kFold2Units * (double)a.nfibs[a.S - 2]) f = 1;
+  return f;
+}
 
 // The (V, W, VW) shapes the contraction is built for: V columns per lane in
 // the level loop (32 lanes cover the rank), W walkers in the source loop
@@ -1174,16 +1212,17 @@ int walker_cols(int R, int W) {
 }
 
 template <FactorType FT, bool LEAF>
-void launch_contract(int vec, int walkers, const WalkArgs &a, unsigned blocks, bool resident,
+void launch_contract(int vec, int walkers, int fold, const WalkArgs &a, unsigned blocks, bool resident,
                      cudaStream_t s) {
-  const bool fuse = fusable(a);
+  const int f = fold_levels(a, fold);
   const int vw = walker_cols(a.R, walkers);
-#define ADATM_CONTRACT_CASE(V, W, VW)                                              \
-  if (vec == V && walkers == W && vw == VW) {                                      \
-    if (fuse) launch_contract_v<V, W, VW, FT, LEAF, true>(a, blocks, resident, s); \
-    else launch_contract_v<V, W, VW, FT, LEAF, false>(a, blocks, resident, s);     \
-    ADATM_LAUNCH();                                                                \
-    return;                                                                        \
+#define ADATM_CONTRACT_CASE(V, W, VW)                                                  \
+  if (vec == V && walkers == W && vw == VW) {                                          \
+    if (f == 2) launch_contract_v<V, W, VW, FT, LEAF, 2>(a, blocks, resident, s);      \
+    else if (f == 1) launch_contract_v<V, W, VW, FT, LEAF, 1>(a, blocks, resident, s); \
+    else launch_contract_v<V, W, VW, FT, LEAF, 0>(a, blocks, resident, s);             \
+    ADATM_LAUNCH();                                                                    \
+    return;                                                                            \
   }
   ADATM_CONTRACT_SHAPES(ADATM_CONTRACT_CASE)
 #undef ADATM_CONTRACT_CASE
@@ -1255,13 +1294,14 @@ int lanes_for_rank(int R) {
 void set_walk_attributes() {
   static bool done = false;
   if (done) return;
-#define ADATM_ATTR_C1(V, W, VW, FT, LEAF)                                         \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, W, VW, FT, LEAF, false>,          \
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,    \
-                                  (int)contract_smem<V>(kMaxModes)));             \
-  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, W, VW, FT, LEAF, true>,           \
+#define ADATM_ATTR_C0(V, W, VW, FT, LEAF, F)                                      \
+  ADATM_CUDA(cudaFuncSetAttribute(k_contract<V, W, VW, FT, LEAF, F>,              \
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,    \
                                   (int)contract_smem<V>(kMaxModes)));
+#define ADATM_ATTR_C1(V, W, VW, FT, LEAF) \
+  ADATM_ATTR_C0(V, W, VW, FT, LEAF, 0)    \
+  ADATM_ATTR_C0(V, W, VW, FT, LEAF, 1)    \
+  ADATM_ATTR_C0(V, W, VW, FT, LEAF, 2)
 #define ADATM_ATTR_CS(V, W, VW)                       \
   ADATM_ATTR_C1(V, W, VW, FactorType::F32, true)      \
   ADATM_ATTR_C1(V, W, VW, FactorType::F32, false)     \
@@ -1289,6 +1329,7 @@ void set_walk_attributes() {
 #undef ADATM_ATTR_S
 #undef ADATM_ATTR_CS
 #undef ADATM_ATTR_C1
+#undef ADATM_ATTR_C0
   done = true;
 }
 
@@ -1624,11 +1665,11 @@ void walk_launch(const TreeWalk &w, const LevelFactors &f, FactorType ft, double
     const int vec = vec_for_rank(w.R);
     const int wk = w.walkers > 0 ? w.walkers : default_walkers(w.R);
     if (ft == FactorType::F32) {
-      if (leaf) launch_contract<FactorType::F32, true>(vec, wk, a, blocks, w.resident, s);
-      else launch_contract<FactorType::F32, false>(vec, wk, a, blocks, w.resident, s);
+      if (leaf) launch_contract<FactorType::F32, true>(vec, wk, w.fold, a, blocks, w.resident, s);
+      else launch_contract<FactorType::F32, false>(vec, wk, w.fold, a, blocks, w.resident, s);
     } else {
-      if (leaf) launch_contract<FactorType::BF16, true>(vec, wk, a, blocks, w.resident, s);
-      else launch_contract<FactorType::BF16, false>(vec, wk, a, blocks, w.resident, s);
+      if (leaf) launch_contract<FactorType::BF16, true>(vec, wk, w.fold, a, blocks, w.resident, s);
+      else launch_contract<FactorType::BF16, false>(vec, wk, w.fold, a, blocks, w.resident, s);
     }
     launch_chains(w, out, s);
     if (w.deterministic && w.out > 0) launch_pull(w, f, ft, w.level_rows.get(), out, s);

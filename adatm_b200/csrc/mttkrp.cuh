@@ -51,6 +51,9 @@ struct TreeWalk {
                                              // chunks (else one chunk per warp)
   int walkers = 0;                           // contraction source loop: walkers per warp
                                              // (1, 2 or 4; 0 = default_walkers(R))
+  int fold = -1;                             // contraction: unstored levels below the
+                                             // source folded into its loop (0..2; -1 =
+                                             // chosen from the tree's fan-out)
   // Scatter walks: the output rows that the most units hit (at most
   // kHotRows, each hit by at least kHotMin units) are summed per block in
   // shared memory; hot_slot maps an output row to its slot (0xFF = none).

@@ -2,7 +2,7 @@
 
     python -m adatm_b200.profile_case [--nnz 8000000] [--sweeps 3] [--dims 5000,5000,2000,500]
                                       [--alpha 1.1] [--rank 32] [--bf16] [--plain] [--lognormal]
-                                      [--groups JSON] [--walkers W] [--atomic] [--time]
+                                      [--groups JSON] [--walkers W] [--fold F] [--atomic] [--time]
 
 Builds the tensor, the analytic plan (the plain one-tree-per-mode plan with
 --plain, or the given group list) and the engine on device 0, then runs the given number of sweeps
@@ -30,6 +30,7 @@ def main():
                     help="the plan's group list as JSON (memo_mode, begin_imten, n_imten, o_opt "
                          "per group) instead of the analytic plan")
     ap.add_argument("--walkers", type=int, default=0, help="walkers per warp (0 = default)")
+    ap.add_argument("--fold", type=int, default=-1, help="levels folded into the source loop (-1 = chosen)")
     ap.add_argument("--atomic", action="store_true", help="atomic scatters (not deterministic)")
     a = ap.parse_args()
     dims = [int(x) for x in a.dims.split(",")]
@@ -44,6 +45,8 @@ def main():
     e = A.Engine(t, a.rank, plan, bf16=a.bf16, chunk_leaf=a.chunk, chunk_rows=a.chunk)
     if a.walkers:
         e.set_walkers(a.walkers)
+    if a.fold != -1:
+        e.set_fold(a.fold)
     if a.atomic:
         e.set_deterministic(False)
     e.init_factors(0)

@@ -316,6 +316,15 @@ int adatm_engine_set_resident_grid(adatm_engine *e, int on);
  * counterpart (a launch-shape control). */
 int adatm_engine_set_walkers(adatm_engine *e, int walkers);
 
+/* Unstored tree levels folded into the contraction walks' source loop: 0, 1
+ * or 2 (-1, the default: level S-1 whenever it can be, level S-2 too where
+ * its nodes hold at most 4 source units on average). A folded level's nodes
+ * are not formed: each source unit is multiplied by its ancestors' factor
+ * rows directly. Refused with SPLATT_ERROR_BADINPUT outside -1..2. Results
+ * agree up to FP32 summation order. Drops a captured sweep. No reference
+ * counterpart (a kernel-shape control). */
+int adatm_engine_set_fold(adatm_engine *e, int fold);
+
 /* Deterministic accumulation, on by default (on != 0): no float atomics
  * anywhere in the MTTKRPs. Contractions write the partial sums of the tree
  * nodes that chunk boundaries cut to per-chunk rows and sum them per node in

@@ -197,3 +197,57 @@ def test_walker_split(gpu, R, walkers):
                 assert rel_err(e.mttkrp(m), want) < TOL_F32, (m, chunk)
                 assert rel_err(e.mttkrp_direct(m), want) < TOL_F32, (m, chunk)
             e.free()
+
+
+@pytest.mark.parametrize("R", [16, 32, 64])
+@pytest.mark.parametrize("fold", [0, 1, 2])
+@pytest.mark.parametrize("shape", [([40, 30, 25, 20, 12], 30000), ([900, 700, 500, 300, 200], 40000)])
+def test_folded_levels(gpu, R, fold, shape):
+    """Contractions with 0, 1 or 2 unstored levels folded into the source
+    loop (each unit multiplied by its ancestors' rows) give the oracle's
+    MTTKRP sequence on the plain all-mode plan (leaf-to-root walks with no
+    stores, where two levels fold), the one-mode plan (folded walks that end
+    below the root) and on memo plans, with chunks that cut
+    nodes at every level, deterministic and atomic, at every walker count
+    that covers the rank."""
+    A = gpu
+    dims, nnz = shape
+    inds, vals, dims = draw_coo(dims, nnz, 23, 1.2)
+    ci, cv, cd = O.coo_clean(inds, vals, dims)
+    cd = [int(x) for x in cd]
+    t = A.Tensor.from_coo(ci, cv, cd)
+    _, cands, _ = A.plan_analytic(t, R)
+    plans = [A.plan_splatt(t, A.CSF_ALLMODE), A.plan_splatt(t, A.CSF_ONEMODE)]
+    plans += [{"nmodes": c["nmodes"], "groups": c["groups"]} for c in cands[:2]]
+    mats = O.init_factors(cd, R, 4)
+    walkers = [w for w in (1, 2, 4) if (32 // w) * 4 >= R]
+    for p, plan in enumerate(plans):
+        om = O.Model(ci, cv, cd, R, plan["groups"]) if "use_csfs" not in plan else None
+        for chunk in (0, 7):
+            for det in (True, False):
+                e = A.Engine(t, R, plan, chunk_leaf=chunk, chunk_rows=chunk)
+                e.set_fold(fold)
+                e.set_deterministic(det)
+                e.set_walkers(walkers[(p + chunk) % len(walkers)])
+                e.set_factors(mats)
+                for m in range(5):
+                    if om is not None:
+                        want = om.mttkrp(mats, m)
+                    else:
+                        g = plan["use_csfs"][m]
+                        want = O.mttkrp_csf(ci, cv, cd, plan["groups"][g]["o_opt"], mats, m, R)
+                    assert rel_err(e.mttkrp(m), want) < TOL_F32, (p, m, chunk, det)
+                e.free()
+
+
+def test_fold_refused(gpu):
+    """Fold counts outside -1..2 are refused."""
+    A = gpu
+    inds, vals, dims = draw_coo([40, 30, 25], 3000, 5, 1.2)
+    ci, cv, cd = O.coo_clean(inds, vals, dims)
+    t = A.Tensor.from_coo(ci, cv, [int(x) for x in cd])
+    e = A.Engine(t, 16, A.plan_splatt(t, A.CSF_ALLMODE))
+    for bad in (-2, 3):
+        with pytest.raises(A.AdatmError):
+            e.set_fold(bad)
+    e.free()
