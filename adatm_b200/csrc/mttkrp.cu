@@ -405,8 +405,12 @@ __global__ void __launch_bounds__(256, contract_min_blocks<V>())
     // open node of level `top` carried in from earlier batches (every walker
     // holds the same copy)
     fv<VW> acc = fv_fill<VW>(0.f);
-    // unit rows in flight per lane, never more than the walker's segment
-    constexpr int SB = ((F ? 8 : 16) / VW) < SEG ? ((F ? 8 : 16) / VW) : SEG;
+    // unit rows in flight per lane, never more than the walker's segment:
+    // fewer as each unit gathers more rows (the 64 registers a thread has at
+    // four blocks per SM are the limit; spilling costs more than the extra
+    // load latency exposed)
+    constexpr int SB0 = (F == 2 ? 4 : (F == 1 ? 8 : 16)) / VW;
+    constexpr int SB = SB0 < SEG ? SB0 : SEG;
     static_assert(SEG % SB == 0, "a walker's segment is a whole number of load groups");
     const uint64_t u0 = (uint64_t)chunk_id * a.chunk;
     const uint64_t u1 = min(u0 + a.chunk, a.nunits);
