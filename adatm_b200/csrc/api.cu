@@ -290,15 +290,24 @@ Engine &caller_engine(CsfHandle &h, rcsf_seq_adaptive const *rs_seq, idx_t n_csf
 
 // The ALS loop shared by the splatt_* entry points, with the reference's
 // per-iteration report (adatm_cpd.c:343-354).
-double run_als(Engine &e, uint64_t niters, double tol, int verbosity) {
+// With `out`, the last iteration's factors come back normalised into `out`
+// and `lambda` while that sweep runs (Engine::sweep_download) and
+// *downloaded is set; a tolerance stop before it leaves them on the device.
+double run_als(Engine &e, uint64_t niters, double tol, int verbosity, double *const *out = nullptr,
+               double *lambda = nullptr, bool *downloaded = nullptr) {
   e.als_begin();
   e.capture_graph();  // one sweep as a CUDA graph, reused across calls
   double fit = 0, old = 0;
   const auto t0 = std::chrono::steady_clock::now();
   for (uint64_t it = 0; it < niters; ++it) {
     const auto ti = std::chrono::steady_clock::now();
-    e.sweep();
-    fit = e.fit_host();
+    if (out != nullptr && it + 1 == niters) {
+      fit = e.sweep_download(out, lambda);
+      *downloaded = true;
+    } else {
+      e.sweep();
+      fit = e.fit_host();
+    }
     if (verbosity > SPLATT_VERBOSITY_NONE) {
       const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - ti).count();
       printf("  its = %3" PRIu64 " (%0.3fs)  fit = %0.5f  delta = %+0.4e\n", it + 1, s, fit,
@@ -834,9 +843,10 @@ double cpd_als_iterate_adaptive(splatt_csf const *const tensors, rcsf_seq_adapti
       om[m] = mats[m]->vals;
     }
     e.set_factors(fm);
+    bool downloaded = false;
     fit = run_als(e, (uint64_t)opts[SPLATT_OPTION_NITER], opts[SPLATT_OPTION_TOLERANCE],
-                  (int)opts[SPLATT_OPTION_VERBOSITY]);
-    e.get_normalized(om, lambda);
+                  (int)opts[SPLATT_OPTION_VERBOSITY], om, lambda, &downloaded);
+    if (!downloaded) e.get_normalized(om, lambda);
   });
   if (rc != SPLATT_SUCCESS) {
     fprintf(stderr, "cpd_als_iterate_adaptive: %s\n", g_last_error.c_str());

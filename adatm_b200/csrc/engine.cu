@@ -136,6 +136,9 @@ Engine::Engine(std::shared_ptr<const DevCoo> coo, std::vector<std::shared_ptr<De
   ADATM_CUDA(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming));
   ADATM_CUDA(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming));
   ADATM_CUDA(cudaEventCreateWithFlags(&staged_, cudaEventDisableTiming));
+  ADATM_CUDA(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+  for (auto &ev : updated_) ADATM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  for (auto &ev : landed_) ADATM_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   build_walks();
   ADATM_CUDA(cudaStreamSynchronize(stream_));
 }
@@ -146,6 +149,12 @@ Engine::~Engine() {
   if (join_) cudaEventDestroy(join_);
   if (fork_) cudaEventDestroy(fork_);
   if (staged_) cudaEventDestroy(staged_);
+  if (copy_) cudaStreamSynchronize(copy_);
+  for (auto ev : updated_)
+    if (ev) cudaEventDestroy(ev);
+  for (auto ev : landed_)
+    if (ev) cudaEventDestroy(ev);
+  if (copy_) cudaStreamDestroy(copy_);
   if (side_) cudaStreamDestroy(side_);
   if (staging_) cudaFreeHost(staging_);
 }
@@ -608,6 +617,60 @@ void Engine::get_normalized(double *const *host, double *lambda) {
   }
 }
 
+double Engine::sweep_download(double *const *host, double *lambda) {
+  const int N = coo_->nmodes;
+  sweep();
+  size_t total = 0;
+  for (int m = 0; m < N; ++m) total += (size_t)coo_->dims[m] * ldr_;
+  // the same staging layout as get_normalized: rows, then Grams and lambda
+  const size_t extra = 2 * ((size_t)N * R_ * R_ + R_);
+  float *buf = staging(total + extra);
+  double *diag = reinterpret_cast<double *>(buf + total);
+  double *lam = diag + (size_t)N * R_ * R_;
+  size_t off = 0;
+  for (int m = 0; m < N; ++m) {
+    ADATM_CUDA(cudaStreamWaitEvent(copy_, updated_[m], 0));
+    ADATM_CUDA(cudaMemcpyAsync(buf + off, A_[m].get(), (size_t)coo_->dims[m] * ldr_ * sizeof(float),
+                               cudaMemcpyDeviceToHost, copy_));
+    ADATM_CUDA(cudaMemcpyAsync(diag + (size_t)m * R_ * R_, G_[m].get(), R_ * R_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, copy_));
+    ADATM_CUDA(cudaEventRecord(landed_[m], copy_));
+    off += (size_t)coo_->dims[m] * ldr_;
+  }
+  // lambda is final after the last mode's update, which the copy stream
+  // has waited for
+  ADATM_CUDA(cudaMemcpyAsync(lam, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost, copy_));
+  ADATM_CUDA(cudaEventRecord(landed_[N], copy_));
+  // each mode is normalised as it lands, while the GPU runs the later modes
+  std::vector<double> nrm((size_t)N * R_);
+  off = 0;
+  for (int m = 0; m < N; ++m) {
+    ADATM_CUDA(cudaEventSynchronize(landed_[m]));
+    const double *G = diag + (size_t)m * R_ * R_;
+    std::vector<double> inv(R_);
+    for (uint64_t r = 0; r < R_; ++r) {
+      const double n = std::sqrt(std::max(G[r * R_ + r], 0.0));
+      nrm[(size_t)m * R_ + r] = n;
+      inv[r] = n > 0 ? 1.0 / n : 0.0;
+    }
+    const uint64_t I = coo_->dims[m];
+    const float *b = buf + off;
+    double *h = host[m];
+    const double *iv = inv.data();
+    const uint64_t R = R_, L = (uint64_t)ldr_;
+    host_rows(I, R, [=](uint64_t i0, uint64_t i1) {
+      for (uint64_t i = i0; i < i1; ++i)
+        for (uint64_t r = 0; r < R; ++r) h[i * R + r] = (double)b[i * L + r] * iv[r];
+    });
+    off += (size_t)I * ldr_;
+  }
+  ADATM_CUDA(cudaEventSynchronize(landed_[N]));
+  std::memcpy(lambda, lam, R_ * sizeof(double));
+  for (int m = 0; m < N; ++m)
+    for (uint64_t r = 0; r < R_; ++r) lambda[r] *= nrm[(size_t)m * R_ + r];
+  return fit_host();
+}
+
 void Engine::get_lambda(double *host) const {
   ADATM_CUDA(cudaMemcpyAsync(host, w_.lambda.get(), R_ * sizeof(double), cudaMemcpyDeviceToHost,
                              stream_));
@@ -641,6 +704,15 @@ void Engine::sweep_eager() {
     ADATM_CUDA(cudaStreamWaitEvent(stream_, join_, 0));
     update_factor(M_.get(), coo_->dims[m], A_[m].get(), Ab_[m].get(), G_[m].get(), m == N - 1, w_,
                   stream_);
+    // mode m's rows and Gram are final for this sweep, so a download may
+    // start here: an event node when the sweep is being captured (the
+    // external flag is refused outside a capture)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    ADATM_CUDA(cudaStreamIsCapturing(stream_, &cap));
+    if (cap == cudaStreamCaptureStatusActive)
+      ADATM_CUDA(cudaEventRecordWithFlags(updated_[m], stream_, cudaEventRecordExternal));
+    else
+      ADATM_CUDA(cudaEventRecord(updated_[m], stream_));
   }
   fit(gs, w_, stream_);
 }

@@ -71,6 +71,11 @@ class Engine {
   // which the sweep keeps current), lambda multiplied by those norms; one
   // pass over the downloaded rows.
   void get_normalized(double *const *host, double *lambda);
+  // One sweep whose result comes back as get_normalized's does, but mode by
+  // mode: each mode's rows and Gram are copied out as soon as its update
+  // ends and normalised on the host while the later modes run. Returns the
+  // sweep's fit.
+  double sweep_download(double *const *host, double *lambda);
   float *factor(int m) { return A_[m].get(); }
 
   // MTTKRP of `mode` following the plan (tags 0/1/2) into out (dims x ldr
@@ -190,6 +195,12 @@ class Engine {
   cudaEvent_t fork_ = nullptr, join_ = nullptr;
   cudaEvent_t staged_ = nullptr;  // after the last copy that reads the staging rows
   bool staged_pending_ = false;
+  // Downloads that overlap a sweep: each mode's update records updated_[m]
+  // (an event node of the captured sweep); the copy stream takes the mode's
+  // rows and Gram once it fires and records landed_[m] (landed_[N]: lambda).
+  cudaStream_t copy_ = nullptr;
+  cudaEvent_t updated_[kMaxModes] = {};
+  cudaEvent_t landed_[kMaxModes + 1] = {};
 };
 
 // Many independent tensors swept together: one CUDA graph holds one ALS

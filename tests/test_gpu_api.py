@@ -191,3 +191,28 @@ def test_caller_plan_mismatch_rejected(gpu, name):
     res = A.cpd_als_iterate_adaptive(cs, rs, groups, duc, dut, mats, 5, 0.0, opts)
     assert abs(res["fit"] - float(d["als5_fit"])) < 1e-4
     cs.free()
+
+
+def test_overlapped_download_is_the_plain_download(gpu):
+    """cpd_als_iterate_adaptive copies the last sweep's factors out mode by
+    mode while the sweep runs. Two sweeps that way must give the factors,
+    lambda and fit of three allowed sweeps stopped by the tolerance after two
+    (whose factors come back after the sweep), bit for bit."""
+    A = gpu
+    name = golden_cases()[0]
+    d = load_golden(name)
+    N, R = d["N"], int(d["R"])
+    groups = A.decide_parameters_auto(d["inds"], d["vals"], d["dims_list"], R)
+    cs = A.csf_alloc_adaptive(d["inds"], d["vals"], d["dims_list"], groups)
+    rs = A.rcsf_alloc_adaptive(cs, R, groups)
+    uc, ut = A.decide_use_csfs(N, groups, len(cs))
+    mats = O.init_factors(d["dims_list"], R, 2)
+    a = A.CpdIterator(cs, rs, groups, uc, ut, mats)
+    fa = a.step(2, 0.0)
+    b = A.CpdIterator(cs, rs, groups, uc, ut, mats)
+    fb = b.step(3, 1e9)
+    assert fa == fb
+    for m in range(N):
+        assert a.factors[m].tobytes() == b.factors[m].tobytes(), m
+    assert a.lam.tobytes() == b.lam.tobytes()
+    cs.free()
