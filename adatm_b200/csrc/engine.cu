@@ -51,7 +51,7 @@ class HostPool {
  private:
   HostPool() {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    nworkers_ = std::min(7u, hw > 1 ? hw - 1 : 0u);
+    nworkers_ = std::min(15u, hw > 1 ? hw - 1 : 0u);
     for (unsigned t = 0; t < nworkers_; ++t) std::thread([this] { loop(); }).detach();
   }
   void loop() {
@@ -80,7 +80,7 @@ class HostPool {
 // Rows [0, rows) of a host conversion, split over the pool when large.
 template <typename F>
 void host_rows(uint64_t rows, uint64_t row_elems, F &&f) {
-  const unsigned parts = (unsigned)std::min<uint64_t>(8, rows * row_elems / 32768 + 1);
+  const unsigned parts = (unsigned)std::min<uint64_t>(16, rows * row_elems / 32768 + 1);
   HostPool::instance().run(rows, parts, std::function<void(uint64_t, uint64_t)>(f));
 }
 
@@ -528,13 +528,22 @@ void Engine::init_factors(uint64_t seed) {
 }
 
 void Engine::set_factors(const double *const *host) {
-  size_t total = 0;
-  for (int m = 0; m < coo_->nmodes; ++m) total += (size_t)coo_->dims[m] * ldr_;
+  const int N = coo_->nmodes;
+  size_t total = 0, offs[kMaxModes];
+  for (int m = 0; m < N; ++m) {
+    offs[m] = total;
+    total += (size_t)coo_->dims[m] * ldr_;
+  }
   float *buf = staging(total);
-  size_t off = 0;
-  for (int m = 0; m < coo_->nmodes; ++m) {
+  // largest mode first: each mode's copy runs while the next is converted,
+  // so the sweep waits only on the last (smallest) one
+  int order[kMaxModes];
+  for (int m = 0; m < N; ++m) order[m] = m;
+  std::stable_sort(order, order + N, [&](int x, int y) { return coo_->dims[x] > coo_->dims[y]; });
+  for (int k = 0; k < N; ++k) {
+    const int m = order[k];
     const uint64_t I = coo_->dims[m];
-    float *b = buf + off;
+    float *b = buf + offs[m];
     const double *h = host[m];
     const uint64_t R = R_, L = (uint64_t)ldr_;
     host_rows(I, L, [=](uint64_t i0, uint64_t i1) {
@@ -546,7 +555,6 @@ void Engine::set_factors(const double *const *host) {
     ADATM_CUDA(cudaMemcpyAsync(A_[m].get(), b, (size_t)I * ldr_ * sizeof(float),
                                cudaMemcpyHostToDevice, stream_));
     if (Ab_[m].get()) to_bf16(A_[m].get(), Ab_[m].get(), I, ldr_, stream_);
-    off += (size_t)I * ldr_;
   }
   // the copies run on; the staging rows are not reused before they end
   ADATM_CUDA(cudaEventRecord(staged_, stream_));
